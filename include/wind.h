@@ -1,0 +1,188 @@
+/*
+ * wind.h -- C ABI of the B200 batched stiff-ODE integrators (SIE and RK2).
+ *
+ * Two layers are exported:
+ *
+ *  1. The drop-in entry of the reference solver libraries (declared in
+ *     wind_legacy.h): `cudaIntegrateSystem`, with the reference's C++ linkage
+ *     and signature (cuda/common/harness.cu:5-14), so the reference's ctypes
+ *     caller (python/wind_harness.py:32-40, python/ode_systems/ode_base.py:441-469)
+ *     and its dlopen driver (cuda/debug/debug.c:14-17) bind it unchanged.
+ *
+ *  2. The extern "C" API below: FP64 state, explicit constants stride,
+ *     per-system status and step counts, a stream, and a choice of linear
+ *     solver.  It replaces the same call (cuda/common/harness.cu:5-106) with
+ *     the information the legacy signature cannot carry.
+ *
+ * Every function returns a wind_status code; none aborts or traps.
+ *
+ * Layouts (the reference's own, cuda/common/kernel.cu:264-273):
+ *   y[s*N + i]                      state, array-of-structures per system
+ *   constants[s*n_const + k]        per-system constants
+ *   rates[s*R + r], species[(s*R + r)*4 + q]  mass-action reactions
+ *   linear[(s*N + j)*N + k]         dense linear term, f_j += L_jk y_k
+ * The Jacobian handed to solvers is the reference's transposed layout,
+ * Jt[i*N + j] = d f_j / d y_i (cuda/common/kernel.cu:123,
+ * cuda/c_baseline/linear_algebra/matrix_ops.c:16-20).
+ */
+#ifndef WIND_H
+#define WIND_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ------------------------------------------------------ */
+typedef enum wind_status {
+    WIND_OK = 0,
+    WIND_ERR_ARGUMENT = 1,     /* bad pointer, size or enum value            */
+    WIND_ERR_UNSUPPORTED = 2,  /* combination not built (e.g. N too large)   */
+    WIND_ERR_CUDA = 3,         /* a CUDA runtime call failed                 */
+    WIND_ERR_NOMEM = 4,        /* device allocation failed / over the cap    */
+    WIND_ERR_TIMEOUT = 5,      /* host-side wait ran out                     */
+    WIND_ERR_BUSY = 6,         /* admission refused (serving)                */
+    WIND_ERR_NOT_FOUND = 7     /* unknown request id (serving)               */
+} wind_status;
+
+/* ---- per-system status bits (written to sys_status[s]) ----------------- */
+enum {
+    WIND_SYS_OK = 0,
+    WIND_SYS_NONFINITE = 1,      /* state contains NaN/Inf at the end          */
+    WIND_SYS_MAX_ATTEMPTS = 2,   /* attempt budget ran out before tend         */
+    WIND_SYS_STALLED = 4,        /* tnow + h == tnow: step below resolution    */
+    WIND_SYS_REFINE_FALLBACK = 8,/* mixed solve fell back to the FP64 solve    */
+    WIND_SYS_TIMEOUT = 16,       /* device deadline passed                     */
+    WIND_SYS_BAD_INPUT = 32      /* species index >= N: system not integrated  */
+};
+
+/* ---- enums --------------------------------------------------------------- */
+/* Integration method: the reference builds one library per method
+ * (cuda/Makefile:68-73, -DSIE / -DRK2). */
+enum { WIND_METHOD_SIE = 0, WIND_METHOD_RK2 = 1 };
+
+/* Step-doubling controller semantics.
+ * DEVICE: the reference GPU kernel (cuda/common/kernel.cu:12-39, 191-296):
+ *         strict '>' tolerance tests, refinement cap 10 (SIE) / 20 (RK2),
+ *         substep h clamped with fmin, SIE update accumulated term by term.
+ * GOLD:   the reference CPU twin (cuda/c_baseline/common/common_gold.c:8-153):
+ *         '>=' tests, cap 10 for both methods, no clamp, matvec then update. */
+enum { WIND_CTRL_DEVICE = 0, WIND_CTRL_GOLD = 1 };
+
+/* Linear solve inside each SIE substep, (I - hJ) x = f.
+ * GJE_F64: the reference's unpivoted Gauss-Jordan inverse followed by the
+ *          transposed matrix-vector product, in FP64, same operation order
+ *          (cuda/c_baseline/linear_algebra/gje_gold.c:5-144,
+ *           cuda/linear_algebra/gauss_jordan_elimination.cu:15-212).
+ * LU_F64:  partial-pivot LU solve in FP64.
+ * MIXED:   FP32 partial-pivot LU factor, FP64 residual, FP64 iterative
+ *          refinement; falls back to LU_F64 for a system whose refinement
+ *          does not converge (flag WIND_SYS_REFINE_FALLBACK). */
+enum { WIND_SOLVER_GJE_F64 = 0, WIND_SOLVER_LU_F64 = 1, WIND_SOLVER_MIXED = 2 };
+
+/* Network kinds: the ode_system plug-ins (cuda/include/device.h:1-13,
+ * cuda/include/ode_gold.h:1-12).
+ *   NR_TEST    2 equations, 4 constants   (python/ode_systems/NR_test.py:575-603)
+ *   KATZ96     5 equations, 10 constants  (cuda/ode_system/ode_gold.c:3-93)
+ *   STIFFTRIG  2 equations, 2 constants   (python/ode_systems/stifftrig.py:625-661)
+ *   MASS_ACTION runtime network: per-system two-body reactions A+B -> C+D
+ *              with rate k (w = k y_A y_B), plus an optional dense linear
+ *              term L (f += L y).  No reference instance exists; it follows
+ *              the same RHS/Jacobian contract. */
+enum { WIND_NET_NR_TEST = 1, WIND_NET_KATZ96 = 2, WIND_NET_STIFFTRIG = 3,
+       WIND_NET_MASS_ACTION = 4 };
+
+enum { WIND_MEM_HOST = 0, WIND_MEM_DEVICE = 1 };
+
+typedef struct wind_network {
+    int32_t kind;               /* WIND_NET_*                                  */
+    int32_t n_eq;               /* equations per system (N)                    */
+    int32_t n_const;            /* constants per system (builtin kinds)        */
+    int32_t n_react;            /* reactions per system (mass action)          */
+    const double*   constants;  /* [nsys*n_const] or NULL                      */
+    const double*   rates;      /* [nsys*n_react] or NULL                      */
+    const uint16_t* species;    /* [nsys*n_react*4] or NULL                    */
+    const float*    linear;     /* [nsys*N*N] or NULL                          */
+} wind_network;
+
+typedef struct wind_options {
+    int32_t method;             /* WIND_METHOD_*                               */
+    int32_t solver;             /* WIND_SOLVER_*                               */
+    int32_t controller;         /* WIND_CTRL_*                                 */
+    int32_t spec_width;         /* speculative refinement lanes per system,
+                                   1,2,4,8,16 or 32; 0 = tuned default        */
+    int64_t max_attempts;       /* per system per call; 0 = 1<<40              */
+    double  timeout_s;          /* device deadline per call; 0 = none          */
+} wind_options;
+
+/* Fill `opt` with the defaults: SIE, GJE_F64, DEVICE, tuned width. */
+void wind_default_options(wind_options* opt);
+
+/* Integrate nsys independent systems from tnow to tend.
+ * Replaces cudaIntegrateSystem (cuda/common/harness.cu:5-106) with FP64 state.
+ *  y            [nsys*N] in/out
+ *  sys_status   [nsys] out or NULL;  sys_nsteps [nsys] out or NULL
+ *  total_nsteps out or NULL: sum of substeps, 3 per attempt
+ *               (cuda/common/kernel.cu:192, cuda/common/harness.cu:105)
+ *  memory       WIND_MEM_HOST: all arrays are host memory, the call copies
+ *               in and out and returns after the results are back.
+ *               WIND_MEM_DEVICE: all arrays are device memory on the current
+ *               device; the call is asynchronous on `stream` except that
+ *               total_nsteps (a host pointer) forces a synchronisation.
+ *  stream       cudaStream_t, or NULL for the legacy default stream. */
+int wind_integrate(const wind_options* opt, const wind_network* net,
+                   double tnow, double tend, int32_t n_integration_steps,
+                   double* y, int64_t nsys, double atol, double rtol,
+                   int32_t* sys_status, int64_t* sys_nsteps,
+                   int64_t* total_nsteps, int32_t memory, void* stream);
+
+/* ---- mixed-size batch in one persistent launch ------------------------- */
+/* One group = one network shape with its own systems, interval and
+ * tolerances.  All groups of a batch share the method/solver/controller.
+ * All pointers are device pointers. */
+typedef struct wind_group {
+    wind_network net;
+    double*  y;                 /* [nsys*N] in/out (device)                    */
+    int64_t  nsys;
+    double   tnow, tend;
+    int32_t  n_integration_steps;
+    int32_t  pad_;
+    double   atol, rtol;
+    int32_t* sys_status;        /* [nsys] (device) or NULL                     */
+    int64_t* sys_nsteps;        /* [nsys] (device) or NULL                     */
+} wind_group;
+
+/* Integrate all groups in ONE persistent kernel launch fed by a device work
+ * queue (largest systems first).  Asynchronous on `stream`. */
+int wind_integrate_batch(const wind_options* opt, const wind_group* groups,
+                         int32_t ngroups, void* stream);
+
+/* ---- device-resident output loop (the caller loop of
+ * python/ode_systems/ode_base.py:315-397) -------------------------------- */
+/* Integrate n_output_steps intervals of (tend-tnow)/n_output_steps each, with
+ * the state resident on the device; after every interval the state is copied
+ * to out_over_time[(k+1)*nsys*N ...] (host or device memory, `memory` flag
+ * applies to y/out/steps arrays).  out_over_time[0..nsys*N) receives the
+ * initial state.  steps_per_output [n_output_steps] receives the substep sum of
+ * each interval (ode_base.py:341-349).  The interval launches are captured in
+ * one CUDA graph and replayed. */
+int wind_integrate_output_steps(const wind_options* opt, const wind_network* net,
+                                double tnow, double tend,
+                                int32_t n_integration_steps,
+                                int32_t n_output_steps,
+                                double* y, int64_t nsys, double atol, double rtol,
+                                double* out_over_time, int64_t* steps_per_output,
+                                int32_t memory, void* stream);
+
+/* ---- version / diagnostics -------------------------------------------- */
+const char* wind_version(void);
+const char* wind_status_string(int status);
+/* Kernel launches issued by this library since load (all entry points). */
+int64_t wind_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WIND_H */

@@ -1,0 +1,117 @@
+"""Build the native libraries in-tree (sm_100a), and the oracle checkers.
+
+    python -m wind_b200.build            # libwind.so + legacy libraries
+    python -m wind_b200.build --oracle   # also oracle/_build and oracle/_ref
+
+Outputs (git-ignored, shipped with the tree):
+    wind_b200/lib/libwind.so                     extern "C" API (include/wind.h)
+    wind_b200/lib/<network>/{sie,rk2}.so         drop-in cudaIntegrateSystem
+Compilation is incremental on file modification times.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "lib")
+OBJ = os.path.join(HERE, "_build")
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+                "--expt-relaxed-constexpr", "-Xptxas", "-v"]
+
+# translation units of libwind.so
+UNITS = ["api", "batch"]
+
+LEGACY_NETS = {"nr_test": "WIND_NET_NR_TEST", "katz96": "WIND_NET_KATZ96",
+               "stifftrig": "WIND_NET_STIFFTRIG"}
+LEGACY_METHODS = {"sie": "WIND_METHOD_SIE", "rk2": "WIND_METHOD_RK2"}
+
+
+def _deps():
+    return (glob.glob(os.path.join(CSRC, "*")) +
+            [os.path.join(ROOT, "include", "wind.h"), os.path.join(ROOT, "include", "wind_legacy.h")])
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd, log=None):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if log:
+        with open(log, "w") as fh:
+            fh.write(r.stdout + r.stderr)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("build failed: " + " ".join(cmd[:6]) + " ...")
+    return r
+
+
+def build_native(verbose=False):
+    os.makedirs(LIB, exist_ok=True)
+    os.makedirs(OBJ, exist_ok=True)
+    deps = _deps()
+    objs = []
+    for unit in UNITS:
+        obj = os.path.join(OBJ, unit + ".o")
+        objs.append(obj)
+        if _stale(obj, deps):
+            if verbose:
+                print(f"nvcc {unit}.cu", flush=True)
+            _run([NVCC] + FLAGS + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj],
+                 log=os.path.join(OBJ, unit + ".ptxas.log"))
+    libwind = os.path.join(LIB, "libwind.so")
+    if _stale(libwind, objs):
+        _run([NVCC] + ARCH + ["-shared"] + objs + ["-o", libwind, "-lcudart"])
+    for net, netdef in LEGACY_NETS.items():
+        os.makedirs(os.path.join(LIB, net), exist_ok=True)
+        for meth, mdef in LEGACY_METHODS.items():
+            out = os.path.join(LIB, net, f"{meth}.so")
+            if _stale(out, deps + [libwind]):
+                _run([NVCC] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+                      f"-DWIND_LEGACY_NET={netdef}", f"-DWIND_LEGACY_METHOD={mdef}",
+                      os.path.join(CSRC, "legacy.cu"), "-o", out,
+                      "-L" + LIB, "-lwind", "-Xlinker", "-rpath=$ORIGIN/.."])
+    return libwind
+
+
+def build_oracle(reference_dir="/root/reference"):
+    """The CPU checkers: the restatement always; the reference's own
+    c_baseline only when the reference sources are present."""
+    oracle = os.path.join(ROOT, "oracle")
+    _run(["make", "-s", "-C", oracle])
+    if os.path.isdir(os.path.join(reference_dir, "cuda", "c_baseline")):
+        stamp = os.path.join(oracle, "_ref", "sie_gold_katz96_f64.so")
+        srcs = glob.glob(os.path.join(oracle, "plugins", "*.c")) + [os.path.join(oracle, "build_ref.sh")]
+        if _stale(stamp, srcs):
+            env = dict(os.environ, WIND_REFERENCE=reference_dir)
+            r = subprocess.run(["bash", os.path.join(oracle, "build_ref.sh")], env=env,
+                               capture_output=True, text=True)
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise RuntimeError("oracle/build_ref.sh failed")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--oracle", action="store_true")
+    ap.add_argument("-v", action="store_true")
+    a = ap.parse_args()
+    build_native(verbose=a.v)
+    if a.oracle:
+        build_oracle()
+    print("built", os.path.join(LIB, "libwind.so"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,378 @@
+// api.cu -- extern "C" entry points of libwind (include/wind.h).
+//
+// Host side of the integrators: argument checks, device workspace, the
+// kernel dispatch table, launches and copies.  The reference's harness
+// (cuda/common/harness.cu:5-106) did cudaMalloc / copy / launch / copy /
+// cudaFree per call on the default stream and returned an int step count;
+// here allocations are stream-ordered (cudaMallocAsync draws from the
+// device's pool, so repeated calls do not hit the driver), the caller may
+// pass device pointers to skip the copies, and every failure is a status.
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "api_internal.h"
+#include "lane_kernel.cuh"
+#include "team_kernel.cuh"
+
+using namespace wind;
+
+namespace wind {
+
+std::atomic<int64_t> g_launches{0};
+
+static int builtin_n(int kind) {
+    switch (kind) {
+    case WIND_NET_NR_TEST: return NetNR::N;
+    case WIND_NET_KATZ96: return NetKatz96::N;
+    case WIND_NET_STIFFTRIG: return NetTrig::N;
+    default: return -1;
+    }
+}
+static int builtin_nc(int kind) {
+    switch (kind) {
+    case WIND_NET_NR_TEST: return NetNR::NC;
+    case WIND_NET_KATZ96: return NetKatz96::NC;
+    case WIND_NET_STIFFTRIG: return NetTrig::NC;
+    default: return -1;
+    }
+}
+
+// ---- lane kernel dispatch ------------------------------------------------
+using LaneFn = void (*)(KParams, int);
+
+template <class Net, int METHOD, int CTRL>
+static LaneFn lane_by_solver(int solver) {
+    if (METHOD == WIND_METHOD_RK2) return k_lane<Net, METHOD, CTRL, 0>;
+    switch (solver) {
+    case WIND_SOLVER_GJE_F64: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_GJE_F64>;
+    case WIND_SOLVER_LU_F64: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_LU_F64>;
+    default: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_MIXED>;
+    }
+}
+template <class Net>
+static LaneFn lane_for_net(int method, int ctrl, int solver) {
+    if (method == WIND_METHOD_SIE)
+        return ctrl == WIND_CTRL_GOLD ? lane_by_solver<Net, WIND_METHOD_SIE, WIND_CTRL_GOLD>(solver)
+                                      : lane_by_solver<Net, WIND_METHOD_SIE, WIND_CTRL_DEVICE>(solver);
+    return ctrl == WIND_CTRL_GOLD ? lane_by_solver<Net, WIND_METHOD_RK2, WIND_CTRL_GOLD>(solver)
+                                  : lane_by_solver<Net, WIND_METHOD_RK2, WIND_CTRL_DEVICE>(solver);
+}
+static LaneFn lane_kernel(int kind, int method, int ctrl, int solver) {
+    switch (kind) {
+    case WIND_NET_NR_TEST: return lane_for_net<NetNR>(method, ctrl, solver);
+    case WIND_NET_KATZ96: return lane_for_net<NetKatz96>(method, ctrl, solver);
+    case WIND_NET_STIFFTRIG: return lane_for_net<NetTrig>(method, ctrl, solver);
+    default: return nullptr;
+    }
+}
+
+int device_sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
+    return n;
+}
+
+static int lane_blocks_per_sm(LaneFn fn) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void*, int>> cache;
+    std::lock_guard<std::mutex> g(mu);
+    for (auto& e : cache)
+        if (e.first == (const void*)fn) return e.second;
+    int nb = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, LANE_THREADS, 0) != cudaSuccess || nb < 1)
+        nb = 1;
+    cache.push_back({(const void*)fn, nb});
+    return nb;
+}
+
+int choose_width(int64_t nsys, int slots, int method, int ctrl) {
+    const int cap = (ctrl == WIND_CTRL_DEVICE && method == WIND_METHOD_RK2) ? 20 : 10;
+    const int wmax = cap >= 16 ? 32 : 16;
+    int w = 1;
+    while (w < wmax && nsys * (int64_t)(2 * w) <= (int64_t)slots) w *= 2;
+    return w;
+}
+
+wind_status check_network(const wind_network* net, int64_t nsys) {
+    if (!net) return WIND_ERR_ARGUMENT;
+    if (net->kind == WIND_NET_MASS_ACTION) {
+        if (net->n_eq < 1 || net->n_eq > TEAM_MAXN) return WIND_ERR_UNSUPPORTED;
+        if (net->n_react < 0) return WIND_ERR_ARGUMENT;
+        if (nsys > 0 && net->n_react > 0 && (!net->rates || !net->species)) return WIND_ERR_ARGUMENT;
+        return WIND_OK;
+    }
+    const int n = builtin_n(net->kind);
+    if (n < 0) return WIND_ERR_ARGUMENT;
+    if (net->n_eq != n) return WIND_ERR_ARGUMENT;
+    if (net->n_const < builtin_nc(net->kind)) return WIND_ERR_ARGUMENT;
+    if (nsys > 0 && !net->constants) return WIND_ERR_ARGUMENT;
+    return WIND_OK;
+}
+
+// Launch the right kernel family for one homogeneous batch already on the
+// device.  `p.counters` must point at zeroed device counters.
+wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream_t stream) {
+    if (p.nsys == 0) return WIND_OK;
+    if (p.kind != WIND_NET_MASS_ACTION) {
+        LaneFn fn = lane_kernel(p.kind, o.method, o.controller, o.solver);
+        if (!fn) return WIND_ERR_UNSUPPORTED;
+        const int nb = lane_blocks_per_sm(fn);
+        const int slots = nb * device_sm_count() * LANE_THREADS;
+        int w = o.spec_width;
+        if (w <= 0) w = choose_width(p.nsys, slots, o.method, o.controller);
+        if (w != 1 && w != 2 && w != 4 && w != 8 && w != 16 && w != 32) return WIND_ERR_ARGUMENT;
+        const int64_t need = (p.nsys * w + LANE_THREADS - 1) / LANE_THREADS;
+        const int grid = (int)(need < (int64_t)nb * device_sm_count() ? need : (int64_t)nb * device_sm_count());
+        fn<<<grid, LANE_THREADS, 0, stream>>>(p, w);
+        g_launches++;
+        return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
+    }
+    return launch_team(o, p, stream);
+}
+
+}  // namespace wind
+
+// ===========================================================================
+extern "C" {
+
+void wind_default_options(wind_options* opt) {
+    if (!opt) return;
+    opt->method = WIND_METHOD_SIE;
+    opt->solver = WIND_SOLVER_GJE_F64;
+    opt->controller = WIND_CTRL_DEVICE;
+    opt->spec_width = 0;
+    opt->max_attempts = 0;
+    opt->timeout_s = 0.0;
+}
+
+const char* wind_version(void) { return "wind_b200 0.1 (sm_100a)"; }
+
+const char* wind_status_string(int s) {
+    switch (s) {
+    case WIND_OK: return "ok";
+    case WIND_ERR_ARGUMENT: return "invalid argument";
+    case WIND_ERR_UNSUPPORTED: return "unsupported configuration";
+    case WIND_ERR_CUDA: return "CUDA runtime error";
+    case WIND_ERR_NOMEM: return "out of device memory";
+    case WIND_ERR_TIMEOUT: return "timed out";
+    case WIND_ERR_BUSY: return "admission refused";
+    case WIND_ERR_NOT_FOUND: return "unknown request";
+    default: return "unknown status";
+    }
+}
+
+int64_t wind_launch_count(void) { return g_launches.load(); }
+
+int wind_integrate(const wind_options* opt_in, const wind_network* net, double tnow,
+                   double tend, int32_t n_integration_steps, double* y, int64_t nsys,
+                   double atol, double rtol, int32_t* sys_status, int64_t* sys_nsteps,
+                   int64_t* total_nsteps, int32_t memory, void* stream_v) {
+    wind_options o;
+    if (opt_in) o = *opt_in; else wind_default_options(&o);
+    if (o.method != WIND_METHOD_SIE && o.method != WIND_METHOD_RK2) return WIND_ERR_ARGUMENT;
+    if (o.controller != WIND_CTRL_DEVICE && o.controller != WIND_CTRL_GOLD) return WIND_ERR_ARGUMENT;
+    if (o.solver < WIND_SOLVER_GJE_F64 || o.solver > WIND_SOLVER_MIXED) return WIND_ERR_ARGUMENT;
+    if (nsys < 0 || n_integration_steps < 1) return WIND_ERR_ARGUMENT;
+    if (memory != WIND_MEM_HOST && memory != WIND_MEM_DEVICE) return WIND_ERR_ARGUMENT;
+    wind_status st = check_network(net, nsys);
+    if (st != WIND_OK) return st;
+    if (nsys > 0 && !y) return WIND_ERR_ARGUMENT;
+    if (total_nsteps) *total_nsteps = 0;
+    if (nsys == 0) return WIND_OK;
+    cudaStream_t stream = (cudaStream_t)stream_v;
+
+    IntegrateCall call;
+    st = call.prepare(o, *net, tnow, tend, n_integration_steps, y, nsys, atol, rtol,
+                      sys_status, sys_nsteps, memory, stream);
+    if (st == WIND_OK) st = launch_integrate(o, call.params, stream);
+    if (st == WIND_OK) st = call.finish(total_nsteps);
+    call.release();
+    return st;
+}
+
+}  // extern "C"
+
+// ---- team kernel dispatch (mass action, N <= 32) ---------------------------
+namespace wind {
+
+using TeamFn = void (*)(KParams);
+
+template <int NMAX, int METHOD, int CTRL>
+static TeamFn team_by_solver(int solver) {
+    if (METHOD == WIND_METHOD_RK2) return k_team<NMAX, METHOD, CTRL, 0>;
+    switch (solver) {
+    case WIND_SOLVER_GJE_F64: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_GJE_F64>;
+    case WIND_SOLVER_LU_F64: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_LU_F64>;
+    default: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_MIXED>;
+    }
+}
+template <int NMAX>
+static TeamFn team_for_nmax(int method, int ctrl, int solver) {
+    if (method == WIND_METHOD_SIE)
+        return ctrl == WIND_CTRL_GOLD ? team_by_solver<NMAX, WIND_METHOD_SIE, WIND_CTRL_GOLD>(solver)
+                                      : team_by_solver<NMAX, WIND_METHOD_SIE, WIND_CTRL_DEVICE>(solver);
+    return ctrl == WIND_CTRL_GOLD ? team_by_solver<NMAX, WIND_METHOD_RK2, WIND_CTRL_GOLD>(solver)
+                                  : team_by_solver<NMAX, WIND_METHOD_RK2, WIND_CTRL_DEVICE>(solver);
+}
+
+int team_nmax(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : 32); }
+
+size_t team_smem_bytes(int n, int R, bool lin) {
+    const int nmax = team_nmax(n);
+    return (size_t)(TEAM_THREADS / nmax) * TeamLayout(nmax, R, lin).bytes;
+}
+
+static int team_blocks_per_sm(TeamFn fn, size_t smem) {
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const void*, size_t>, int>> cache;
+    std::lock_guard<std::mutex> g(mu);
+    for (auto& e : cache)
+        if (e.first.first == (const void*)fn && e.first.second == smem) return e.second;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, TEAM_THREADS, smem) != cudaSuccess || nb < 1)
+        nb = 0;
+    cache.push_back({{(const void*)fn, smem}, nb});
+    return nb;
+}
+
+wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream) {
+    const int nmax = team_nmax(p.n_eq);
+    TeamFn fn = nmax == 8 ? team_for_nmax<8>(o.method, o.controller, o.solver)
+              : nmax == 16 ? team_for_nmax<16>(o.method, o.controller, o.solver)
+                           : team_for_nmax<32>(o.method, o.controller, o.solver);
+    const size_t smem = team_smem_bytes(p.n_eq, p.n_react, p.linear != nullptr);
+    if (smem > 227 * 1024) return WIND_ERR_UNSUPPORTED;
+    const int nb = team_blocks_per_sm(fn, smem);
+    if (nb < 1) return WIND_ERR_UNSUPPORTED;
+    const int teams = TEAM_THREADS / nmax;
+    const int64_t need = (p.nsys + teams - 1) / teams;
+    const int64_t cap = (int64_t)nb * device_sm_count();
+    const int grid = (int)(need < cap ? need : cap);
+    fn<<<grid, TEAM_THREADS, smem, stream>>>(p);
+    g_launches++;
+    return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
+}
+
+}  // namespace wind
+
+// ---- device-resident output loop and multi-group batch ---------------------
+extern "C" {
+
+int wind_integrate_output_steps(const wind_options* opt_in, const wind_network* net, double tnow,
+                                double tend, int32_t n_integration_steps, int32_t n_output_steps,
+                                double* y, int64_t nsys, double atol, double rtol,
+                                double* out_over_time, int64_t* steps_per_output, int32_t memory,
+                                void* stream_v) {
+    wind_options o;
+    if (opt_in) o = *opt_in; else wind_default_options(&o);
+    if (n_output_steps < 1 || n_integration_steps < 1 || nsys < 0) return WIND_ERR_ARGUMENT;
+    if (memory != WIND_MEM_HOST && memory != WIND_MEM_DEVICE) return WIND_ERR_ARGUMENT;
+    wind_status st = check_network(net, nsys);
+    if (st != WIND_OK) return st;
+    if (nsys > 0 && (!y || !out_over_time)) return WIND_ERR_ARGUMENT;
+    if (nsys == 0) return WIND_OK;
+    cudaStream_t stream = (cudaStream_t)stream_v;
+    const int N = net->n_eq;
+    const size_t ybytes = (size_t)nsys * N * sizeof(double);
+
+    IntegrateCall call;
+    st = call.prepare(o, *net, tnow, tend, n_integration_steps, y, nsys, atol, rtol, nullptr,
+                      nullptr, memory, stream);
+    // per-interval counters and the trajectory buffer live on the device
+    unsigned long long* cnt = nullptr;
+    double* traj = nullptr;
+    if (st == WIND_OK) {
+        cnt = static_cast<unsigned long long*>(
+            call.alloc((size_t)n_output_steps * CNT_SLOTS * sizeof(unsigned long long)));
+        traj = (memory == WIND_MEM_DEVICE) ? out_over_time
+                                           : static_cast<double*>(call.alloc(ybytes * (n_output_steps + 1)));
+        if (call.failed) st = WIND_ERR_NOMEM;
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cap = nullptr;
+    if (st == WIND_OK && cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
+        st = WIND_ERR_CUDA;
+    // Order the capture stream after the uploads on `stream`.
+    cudaEvent_t ready = nullptr;
+    if (st == WIND_OK) {
+        cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+        cudaEventRecord(ready, stream);
+        cudaStreamWaitEvent(cap, ready, 0);
+        cudaStreamSynchronize(cap);
+    }
+    // ode_base.py:338-378: intervals [tcur, tcur+dt], tcur += dt
+    if (st == WIND_OK && cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const double dt = (tend - tnow) / n_output_steps;
+        double tcur = tnow;
+        cudaMemsetAsync(cnt, 0, (size_t)n_output_steps * CNT_SLOTS * sizeof(unsigned long long), cap);
+        cudaMemcpyAsync(traj, call.params.y, ybytes, cudaMemcpyDeviceToDevice, cap);
+        for (int k = 0; k < n_output_steps && st == WIND_OK; k++) {
+            KParams p = call.params;
+            p.tnow = tcur;
+            p.tend = tcur + dt;
+            p.h0 = (p.tend - p.tnow) / n_integration_steps;
+            p.counters = cnt + (size_t)k * CNT_SLOTS;
+            st = launch_integrate(o, p, cap);
+            cudaMemcpyAsync(traj + (size_t)(k + 1) * nsys * N, call.params.y, ybytes,
+                            cudaMemcpyDeviceToDevice, cap);
+            tcur += dt;
+        }
+        if (cudaStreamEndCapture(cap, &graph) != cudaSuccess) st = WIND_ERR_CUDA;
+        if (st == WIND_OK && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) st = WIND_ERR_CUDA;
+        if (st == WIND_OK && cudaGraphLaunch(exec, cap) != cudaSuccess) st = WIND_ERR_CUDA;
+        g_launches++;  // the graph launch (its kernel nodes are counted above)
+        if (st == WIND_OK) {
+            cudaEventRecord(ready, cap);
+            cudaStreamWaitEvent(stream, ready, 0);
+        }
+    } else if (st == WIND_OK) {
+        st = WIND_ERR_CUDA;
+    }
+    if (st == WIND_OK) {
+        std::vector<unsigned long long> hc((size_t)n_output_steps * CNT_SLOTS);
+        cudaMemcpyAsync(hc.data(), cnt, hc.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                        stream);
+        if (memory == WIND_MEM_HOST)
+            cudaMemcpyAsync(out_over_time, traj, ybytes * (n_output_steps + 1), cudaMemcpyDeviceToHost,
+                            stream);
+        st = call.finish(nullptr);
+        if (st == WIND_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = WIND_ERR_CUDA;
+        if (st == WIND_OK && steps_per_output) {
+            if (memory == WIND_MEM_HOST) {
+                for (int k = 0; k < n_output_steps; k++)
+                    steps_per_output[k] = (int64_t)hc[(size_t)k * CNT_SLOTS + CNT_STEPS];
+            } else {
+                std::vector<int64_t> tmp(n_output_steps);
+                for (int k = 0; k < n_output_steps; k++)
+                    tmp[k] = (int64_t)hc[(size_t)k * CNT_SLOTS + CNT_STEPS];
+                cudaMemcpy(steps_per_output, tmp.data(), tmp.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
+            }
+        }
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap) {
+        cudaStreamSynchronize(cap);
+        cudaStreamDestroy(cap);
+    }
+    if (ready) cudaEventDestroy(ready);
+    call.release();
+    return st;
+}
+
+}  // extern "C"
+
+extern "C" int wind_integrate_batch(const wind_options* opt_in, const wind_group* groups,
+                                    int32_t ngroups, void* stream_v) {
+    wind_options o;
+    if (opt_in) o = *opt_in; else wind_default_options(&o);
+    if (ngroups < 0 || (ngroups > 0 && !groups)) return WIND_ERR_ARGUMENT;
+    return wind::launch_batch(o, groups, ngroups, (cudaStream_t)stream_v);
+}

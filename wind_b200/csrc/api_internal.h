@@ -1,0 +1,142 @@
+// api_internal.h -- host-side pieces shared by the entry points.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/wind.h"
+#include "common.cuh"
+
+namespace wind {
+
+int device_sm_count();
+wind_status check_network(const wind_network* net, int64_t nsys);
+wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream_t stream);
+wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream);
+
+// One wind_integrate call: device copies of host inputs (when memory is
+// HOST), the counters block, and the kernel parameters.  Allocations are
+// stream-ordered (cudaMallocAsync / cudaFreeAsync) and released in release().
+struct IntegrateCall {
+    KParams params{};
+    cudaStream_t stream = nullptr;
+    int memory = WIND_MEM_HOST;
+    double* h_y = nullptr;
+    int32_t* h_status = nullptr;
+    int64_t* h_nsteps = nullptr;
+    size_t ybytes = 0;
+    void* allocs[10] = {};
+    int nalloc = 0;
+    bool failed = false;
+
+    void* alloc(size_t bytes) {
+        void* p = nullptr;
+        if (bytes == 0) bytes = 16;
+        if (cudaMallocAsync(&p, bytes, stream) != cudaSuccess) { failed = true; return nullptr; }
+        allocs[nalloc++] = p;
+        return p;
+    }
+    template <typename T>
+    const T* upload(const T* host, size_t count) {
+        if (!host || count == 0) return nullptr;
+        T* d = static_cast<T*>(alloc(count * sizeof(T)));
+        if (!d) return nullptr;
+        if (cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+            failed = true;
+        return d;
+    }
+
+    wind_status prepare(const wind_options& o, const wind_network& net, double tnow, double tend,
+                        int32_t n_integration_steps, double* y, int64_t nsys, double atol,
+                        double rtol, int32_t* sys_status, int64_t* sys_nsteps, int32_t mem,
+                        cudaStream_t s) {
+        stream = s;
+        memory = mem;
+        const int N = net.n_eq;
+        KParams& p = params;
+        p.kind = net.kind;
+        p.n_eq = N;
+        p.n_const = net.n_const;
+        p.n_react = net.n_react;
+        p.tnow = tnow;
+        p.tend = tend;
+        // cuda/common/harness.cu:80, cuda/c_baseline/sie/sie_gold.c:105
+        p.h0 = (tend - tnow) / n_integration_steps;
+        p.atol = atol;
+        p.rtol = rtol;
+        p.nsys = nsys;
+        p.max_attempts = o.max_attempts > 0 ? o.max_attempts : ((int64_t)1 << 40);
+        p.timeout_ns = o.timeout_s > 0 ? (uint64_t)(o.timeout_s * 1e9) : 0;
+        p.counters = static_cast<unsigned long long*>(alloc(CNT_SLOTS * sizeof(unsigned long long)));
+        if (failed) return WIND_ERR_NOMEM;
+        if (cudaMemsetAsync(p.counters, 0, CNT_SLOTS * sizeof(unsigned long long), stream) != cudaSuccess)
+            return WIND_ERR_CUDA;
+        if (mem == WIND_MEM_DEVICE) {
+            p.constants = net.constants;
+            p.rates = net.rates;
+            p.species = net.species;
+            p.linear = net.linear;
+            p.y = y;
+            p.sys_status = sys_status;
+            p.sys_nsteps = sys_nsteps;
+            return WIND_OK;
+        }
+        // host memory: validate mass-action species indices before upload
+        if (net.kind == WIND_NET_MASS_ACTION && net.species) {
+            const size_t cnt = (size_t)nsys * net.n_react * 4;
+            for (size_t i = 0; i < cnt; i++)
+                if (net.species[i] >= (uint16_t)N) return WIND_ERR_ARGUMENT;
+        }
+        h_y = y;
+        h_status = sys_status;
+        h_nsteps = sys_nsteps;
+        ybytes = (size_t)nsys * N * sizeof(double);
+        p.constants = upload(net.constants, net.constants ? (size_t)nsys * net.n_const : 0);
+        p.rates = upload(net.rates, net.rates ? (size_t)nsys * net.n_react : 0);
+        p.species = upload(net.species, net.species ? (size_t)nsys * net.n_react * 4 : 0);
+        p.linear = upload(net.linear, net.linear ? (size_t)nsys * N * N : 0);
+        p.y = static_cast<double*>(alloc(ybytes));
+        if (failed) return WIND_ERR_NOMEM;
+        if (cudaMemcpyAsync(p.y, y, ybytes, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+            return WIND_ERR_CUDA;
+        if (sys_status) p.sys_status = static_cast<int32_t*>(alloc(nsys * sizeof(int32_t)));
+        if (sys_nsteps) p.sys_nsteps = static_cast<int64_t*>(alloc(nsys * sizeof(int64_t)));
+        if (failed) return WIND_ERR_NOMEM;
+        return WIND_OK;
+    }
+
+    wind_status finish(int64_t* total) {
+        unsigned long long cnt[CNT_SLOTS] = {};
+        if (memory == WIND_MEM_HOST) {
+            if (cudaMemcpyAsync(h_y, params.y, ybytes, cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+                return WIND_ERR_CUDA;
+            if (h_status &&
+                cudaMemcpyAsync(h_status, params.sys_status, params.nsys * sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+                return WIND_ERR_CUDA;
+            if (h_nsteps &&
+                cudaMemcpyAsync(h_nsteps, params.sys_nsteps, params.nsys * sizeof(int64_t),
+                                cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+                return WIND_ERR_CUDA;
+        }
+        if (memory == WIND_MEM_HOST || total) {
+            if (cudaMemcpyAsync(cnt, params.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+                return WIND_ERR_CUDA;
+            if (cudaStreamSynchronize(stream) != cudaSuccess) return WIND_ERR_CUDA;
+            if (total) *total = (int64_t)cnt[CNT_STEPS];
+        }
+        return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
+    }
+
+    void release() {
+        for (int i = 0; i < nalloc; i++) cudaFreeAsync(allocs[i], stream);
+        nalloc = 0;
+    }
+};
+
+}  // namespace wind
+
+namespace wind {
+wind_status launch_batch(const wind_options& o, const wind_group* groups, int ngroups,
+                         cudaStream_t stream);
+}
