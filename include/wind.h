@@ -158,6 +158,25 @@ typedef struct wind_group {
 int wind_integrate_batch(const wind_options* opt, const wind_group* groups,
                          int32_t ngroups, void* stream);
 
+/* ---- allocation-free batch ---------------------------------------------- */
+/* No counterpart in the reference (its harness allocates and frees on every
+ * call, cuda/common/harness.cu:28-58,95-102).  For callers that cannot call
+ * cudaMalloc -- codes whose device memory belongs to another allocator or
+ * budget -- this runs the same kernels as wind_integrate_batch without
+ * allocating: the per-group counters the kernels need live in a static
+ * device array of WIND_NOALLOC_MAX_GROUPS*4 64-bit words (8 KiB, held by
+ * every GPU that loads the library until exit).  All pointers in `groups`
+ * are device pointers.  ngroups > WIND_NOALLOC_MAX_GROUPS returns
+ * WIND_ERR_ARGUMENT.  Groups run one after another on `stream`.  The array
+ * is shared by every call and keeps the last call's contents; each call
+ * clears what it uses first, so calls in sequence are independent, while
+ * calls that overlap on the GPU race and must not be issued.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress);
+ * make it before any stream capture on that device. */
+#define WIND_NOALLOC_MAX_GROUPS 256
+int wind_integrate_batch_noalloc(const wind_options* opt, const wind_group* groups,
+                                 int32_t ngroups, void* stream);
+
 /* ---- device-resident output loop (the caller loop of
  * python/ode_systems/ode_base.py:315-397) -------------------------------- */
 /* Integrate n_output_steps intervals of (tend-tnow)/n_output_steps each, with

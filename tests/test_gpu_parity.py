@@ -73,3 +73,13 @@ def test_fast_solvers_close(cuda_device, wl, solver):
     y_g = wl.y0.copy()
     lib.integrate(wl.net, y_g, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", solver, "device")
     assert mixed_err(y_g, y_o, wl.atol) <= 1e-5
+
+
+def test_batch_matches_single_calls(cuda_device):
+    """wind_integrate_batch (several shapes at once) equals one call per shape."""
+    groups = [CASES[1]] + [c for c in CASES if c.net.kind == W.NET_MASS_ACTION][:2]
+    got = lib.integrate_batch(groups, "sie", "gje_f64", "device")
+    for (yg, sg, ng), wl in zip(got, groups):
+        y = wl.y0.copy()
+        lib.integrate(wl.net, y, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", "gje_f64", "device")
+        assert np.array_equal(yg, y)

@@ -70,6 +70,9 @@ class WindOptions(C.Structure):
     ]
 
 
+NOALLOC_MAX_GROUPS = 256
+
+
 class WindGroup(C.Structure):
     _fields_ = [
         ("net", WindNetwork),
@@ -121,6 +124,9 @@ def declare_api(lib: C.CDLL) -> C.CDLL:
     lib.wind_integrate_batch.argtypes = [C.POINTER(WindOptions), C.POINTER(WindGroup),
                                          C.c_int32, P]
     lib.wind_integrate_batch.restype = C.c_int
+    lib.wind_integrate_batch_noalloc.argtypes = [C.POINTER(WindOptions), C.POINTER(WindGroup),
+                                                 C.c_int32, P]
+    lib.wind_integrate_batch_noalloc.restype = C.c_int
     lib.wind_integrate_output_steps.argtypes = [
         C.POINTER(WindOptions), C.POINTER(WindNetwork), C.c_double, C.c_double,
         C.c_int32, C.c_int32, P, C.c_int64, C.c_double, C.c_double, P, P,

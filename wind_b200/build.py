@@ -27,7 +27,7 @@ FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                 "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 
 # translation units of libwind.so
-UNITS = ["api", "batch"]
+UNITS = ["api", "batch", "noalloc"]
 
 LEGACY_NETS = {"nr_test": "WIND_NET_NR_TEST", "katz96": "WIND_NET_KATZ96",
                "stifftrig": "WIND_NET_STIFFTRIG"}

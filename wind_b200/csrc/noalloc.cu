@@ -1,0 +1,108 @@
+// noalloc.cu -- a batch entry point that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc: host codes whose device memory is
+// owned by another framework's allocator (a hydrodynamics code that hands the
+// integrator slices of its own arena), processes running under a hard device
+// memory budget, and code paths that must not enter the CUDA allocator at all
+// while other work is in flight.  For them, wind_integrate_batch_noalloc runs
+// the same kernels as wind_integrate_batch, but the only global scratch the
+// kernels need -- one small block of counters per group (the work-queue
+// ticket and the substep total) -- lives in the file-scope array below
+// instead of in memory taken from the allocator.  The caller passes every
+// input and output as device memory.
+//
+// Limits and rules:
+//  * at most WIND_NOALLOC_MAX_GROUPS groups per call (the array holds
+//    WIND_NOALLOC_MAX_GROUPS * 4 64-bit counters, 8 KiB); larger calls are
+//    rejected with WIND_ERR_ARGUMENT before anything is launched;
+//  * every GPU that loads this library holds the array until the process
+//    exits;
+//  * the array is shared by all calls on a device and keeps the last call's
+//    contents: each call clears the counters it uses on its stream before its
+//    kernels run, so calls issued one after another are independent, but
+//    calls whose work overlaps on the GPU (different streams, or host threads
+//    racing on one stream) race on the counters and must not be issued;
+//  * the device address of the array is looked up once per device, with that
+//    device current, on the first call made on it; make that first call
+//    before any stream capture on the device;
+//  * the groups run one after another on the caller's stream (no streams or
+//    events are created).
+#include <mutex>
+
+#include "api_internal.h"
+
+namespace {
+
+constexpr int kNoallocSlots = WIND_NOALLOC_MAX_GROUPS * wind::CNT_SLOTS;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned long long g_noalloc_counters[kNoallocSlots];
+
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_counters on the current device (set up once).
+wind_status noalloc_scratch(unsigned long long** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return WIND_ERR_CUDA;
+    if (dev < 0 || dev >= kMaxDevices) return WIND_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_counters);
+        if (e != cudaSuccess || !p) return WIND_ERR_CUDA;
+        g_noalloc_addr[dev] = static_cast<unsigned long long*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return WIND_OK;
+}
+
+}  // namespace
+
+extern "C" int wind_integrate_batch_noalloc(const wind_options* opt_in, const wind_group* groups,
+                                            int32_t ngroups, void* stream_v) {
+    wind_options o;
+    if (opt_in) o = *opt_in; else wind_default_options(&o);
+    if (ngroups < 0 || (ngroups > 0 && !groups)) return WIND_ERR_ARGUMENT;
+    if (ngroups > WIND_NOALLOC_MAX_GROUPS) return WIND_ERR_ARGUMENT;
+    for (int g = 0; g < ngroups; g++) {
+        const wind_status st = wind::check_network(&groups[g].net, groups[g].nsys);
+        if (st != WIND_OK) return st;
+        if (groups[g].nsys > 0 && !groups[g].y) return WIND_ERR_ARGUMENT;
+        if (groups[g].n_integration_steps < 1) return WIND_ERR_ARGUMENT;
+    }
+    if (ngroups == 0) return WIND_OK;
+    cudaStream_t stream = (cudaStream_t)stream_v;
+    unsigned long long* scratch = nullptr;
+    wind_status st = noalloc_scratch(&scratch);
+    if (st != WIND_OK) return st;
+    if (cudaMemsetAsync(scratch, 0, (size_t)ngroups * wind::CNT_SLOTS * sizeof(unsigned long long),
+                        stream) != cudaSuccess)
+        return WIND_ERR_CUDA;
+    for (int g = 0; g < ngroups && st == WIND_OK; g++) {
+        const wind_group& G = groups[g];
+        wind::KParams p{};
+        p.kind = G.net.kind;
+        p.n_eq = G.net.n_eq;
+        p.n_const = G.net.n_const;
+        p.n_react = G.net.n_react;
+        p.constants = G.net.constants;
+        p.rates = G.net.rates;
+        p.species = G.net.species;
+        p.linear = G.net.linear;
+        p.tnow = G.tnow;
+        p.tend = G.tend;
+        p.h0 = (G.tend - G.tnow) / G.n_integration_steps;
+        p.atol = G.atol;
+        p.rtol = G.rtol;
+        p.y = G.y;
+        p.nsys = G.nsys;
+        p.sys_status = G.sys_status;
+        p.sys_nsteps = G.sys_nsteps;
+        p.counters = scratch + (size_t)g * wind::CNT_SLOTS;
+        p.max_attempts = o.max_attempts > 0 ? o.max_attempts : ((int64_t)1 << 40);
+        p.timeout_ns = o.timeout_s > 0 ? (uint64_t)(o.timeout_s * 1e9) : 0;
+        st = wind::launch_integrate(o, p, stream);
+    }
+    return st;
+}

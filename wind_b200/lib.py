@@ -140,6 +140,53 @@ def integrate_output_steps(net: Network, y: np.ndarray, tnow: float, tend: float
     return out, steps
 
 
+class DeviceGroup:
+    """One workload's arrays on the device, kept alive for a batch call."""
+
+    def __init__(self, wl, device):
+        import torch
+        self.wl = wl
+        net = wl.net
+        self.arrays = {k: torch.from_numpy(np.ascontiguousarray(getattr(net, k))).to(device)
+                       for k in ("constants", "rates", "species", "linear")
+                       if getattr(net, k) is not None}
+        self.y = torch.from_numpy(np.ascontiguousarray(wl.y0)).to(device)
+        self.status = torch.zeros(net.nsys, dtype=torch.int32, device=device)
+        self.nsteps = torch.zeros(net.nsys, dtype=torch.int64, device=device)
+
+    def struct(self) -> _capi.WindGroup:
+        wl = self.wl
+        g = _capi.WindGroup()
+        g.net = _capi.network_struct(wl.net, self.arrays)
+        g.y = self.y.data_ptr()
+        g.nsys = wl.net.nsys
+        g.tnow, g.tend = wl.tnow, wl.tend
+        g.n_integration_steps = wl.n_integration_steps
+        g.atol, g.rtol = wl.atol, wl.rtol
+        g.sys_status = self.status.data_ptr()
+        g.sys_nsteps = self.nsteps.data_ptr()
+        return g
+
+
+def integrate_batch(workloads, method="sie", solver="gje_f64", controller="device",
+                    spec_width=0, noalloc=False, device=None, stream=None):
+    """Integrate several workloads (one group each) in one batch call.
+    Returns a list of ``(y, status, nsteps)`` host arrays, one per workload.
+    ``noalloc`` selects wind_integrate_batch_noalloc."""
+    import torch
+    lib = load()
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    groups = [DeviceGroup(wl, device) for wl in workloads]
+    arr = (_capi.WindGroup * max(1, len(groups)))(*[g.struct() for g in groups])
+    o = options(method, solver, controller, spec_width)
+    s = stream if stream is not None else torch.cuda.current_stream(device).cuda_stream
+    fn = lib.wind_integrate_batch_noalloc if noalloc else lib.wind_integrate_batch
+    code = fn(C.byref(o), arr, len(groups), s)
+    _check(code, fn.__name__)
+    torch.cuda.synchronize(device)
+    return [(g.y.cpu().numpy(), g.status.cpu().numpy(), g.nsteps.cpu().numpy()) for g in groups]
+
+
 def legacy(network: str, method: str):
     """The drop-in ``cudaIntegrateSystem`` of ``lib/<network>/<method>.so``,
     bound by the reference's mangled name (python/wind_harness.py:32-40)."""
