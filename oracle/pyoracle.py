@@ -55,6 +55,8 @@ def _load_oracle():
 
 
 def _ranges(nsys, threads):
+    if nsys <= 0:
+        return [(0, 0)]
     threads = max(1, min(threads, nsys))
     edges = np.linspace(0, nsys, threads + 1).astype(np.int64)
     return [(int(edges[i]), int(edges[i + 1])) for i in range(threads) if edges[i + 1] > edges[i]]

@@ -1,0 +1,71 @@
+"""Generate the golden vectors: the reference's own CPU integrator
+(cuda/c_baseline, compiled from the reference sources by oracle/build_ref.sh
+in FP64 with -Dfloat=double) run on small seeded inputs of every network.
+
+    python tests/golden/make_golden.py      # needs oracle/_ref built
+
+Writes tests/golden/golden.npz.  Each case stores the inputs (network arrays,
+y0, interval, tolerances) and the reference outputs (final state, total
+substep count).  The tests compare the oracle restatement and the GPU path
+against these arrays without needing the reference checkout.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import pyoracle as O  # noqa: E402
+from wind_b200 import networks as W  # noqa: E402
+
+
+def cases():
+    out = []
+    nr = W.workload_nr(16, seed=100)
+    out.append(("nr_sie", "sie", W.Workload(nr.net, nr.y0, 0.0, 0.01, 1e-8, 1e-6, 1, 1)))
+    out.append(("nr_rk2", "rk2", W.Workload(nr.net, nr.y0, 0.0, 0.01, 1e-8, 1e-6, 1, 1)))
+    k = W.workload_katz96(32, seed=101)
+    out.append(("katz96_sie", "sie", k))
+    out.append(("katz96_sie_tight", "sie", W.Workload(k.net, k.y0, 0.0, 1e11, 1e-8, 1e-6, 1, 1)))
+    out.append(("katz96_rk2", "rk2", W.Workload(k.net, k.y0, 0.0, 1e6, 5e-3, 5e-3, 1, 1)))
+    t = W.Workload(W.stifftrig(4), np.tile([0.0, 1.0], (4, 1)).astype(np.float64), 0.0, 0.5,
+                   1e-6, 1e-6, 1, 1)
+    out.append(("stifftrig_sie", "sie", t))
+    out.append(("stifftrig_rk2", "rk2", t))
+    rng = np.random.default_rng(102)
+    for n, r, lin in ((3, 6, True), (8, 20, False), (12, 30, True)):
+        net = W.random_mass_action(rng, 6, n, r, 1e-3, 1e1)
+        if lin:
+            net.linear = W.dense_linear(rng, 6, n, 1e-2, 1e3)
+        y0 = rng.uniform(0.0, 1.0, (6, n))
+        wl = W.Workload(net, y0, 0.0, 1e-2, 1e-6, 1e-4, 1, 1)
+        out.append((f"{net.name}_sie", "sie", wl))
+        out.append((f"{net.name}_rk2", "rk2", W.Workload(net, y0, 0.0, 1e-3, 1e-6, 1e-4, 1, 1)))
+    return out
+
+
+def main():
+    blob = {}
+    for name, method, wl in cases():
+        y = wl.y0.copy()
+        tot = O.reference(wl.net, y, wl.tnow, wl.tend, wl.atol, wl.rtol, method,
+                          wl.n_integration_steps)
+        net = wl.net
+        blob[f"{name}/meta"] = np.array([net.kind, net.n_eq, wl.tnow, wl.tend, wl.atol, wl.rtol,
+                                         wl.n_integration_steps, tot], np.float64)
+        blob[f"{name}/method"] = np.array(method)
+        blob[f"{name}/y0"] = wl.y0
+        blob[f"{name}/y"] = y
+        for k in ("constants", "rates", "species", "linear"):
+            a = getattr(net, k)
+            if a is not None:
+                blob[f"{name}/{k}"] = a
+        print(f"{name:24s} {method} substeps={tot}")
+    np.savez_compressed(os.path.join(HERE, "golden.npz"), **blob)
+
+
+if __name__ == "__main__":
+    main()

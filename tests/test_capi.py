@@ -1,0 +1,88 @@
+"""The C ABI without a GPU: the libraries load, every symbol declared in
+include/*.h is exported, argument errors are returned (never trapped) before
+any device work."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from wind_b200 import _capi, lib, networks as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(wind_\w+|cudaIntegrateSystem)\s*\(",
+                                 src, flags=re.M)))
+
+
+def test_libwind_exports_every_declared_symbol():
+    names = _declared("wind.h")
+    assert "wind_integrate" in names and "wind_integrate_batch_noalloc" in names
+    dll = C.CDLL(lib.library_path())
+    for n in names:
+        assert hasattr(dll, n), f"{n} declared in include/wind.h but not exported"
+
+
+@pytest.mark.parametrize("net", ["nr_test", "katz96", "stifftrig"])
+@pytest.mark.parametrize("method", ["sie", "rk2"])
+def test_legacy_libraries_export_reference_symbol(net, method):
+    assert _declared("wind_legacy.h") == ["cudaIntegrateSystem"]
+    fn = lib.legacy(net, method)  # looks up _Z19cudaIntegrateSystemffiPfS_iiff
+    assert fn is not None
+
+
+def test_defaults_and_strings():
+    w = lib.load()
+    o = _capi.WindOptions()
+    w.wind_default_options(C.byref(o))
+    assert (o.method, o.solver, o.controller, o.spec_width) == (0, 0, 0, 0)
+    assert b"sm_100a" in w.wind_version()
+    assert w.wind_status_string(1) == b"invalid argument"
+
+
+def _call(net, y, **kw):
+    w = lib.load()
+    o = lib.options(**kw)
+    ns = _capi.network_struct(net)
+    return w.wind_integrate(C.byref(o), C.byref(ns), 0.0, 1.0, 1, y.ctypes.data if y is not None else None,
+                            net.nsys, 1e-6, 1e-6, None, None, None, _capi.MEM_HOST, None)
+
+
+def test_argument_errors_are_returned():
+    net = W.nr_test(4)
+    y = np.ones((4, 2))
+    w = lib.load()
+    o = lib.options()
+    o.method = 7
+    ns = _capi.network_struct(net)
+    assert w.wind_integrate(C.byref(o), C.byref(ns), 0.0, 1.0, 1, y.ctypes.data, 4, 1e-6, 1e-6,
+                            None, None, None, 0, None) == _capi.WIND_ERR_ARGUMENT
+    # wrong equation count for the builtin network
+    bad = W.Network(W.NET_NR_TEST, 3, 4, constants=net.constants)
+    assert _call(bad, y) == _capi.WIND_ERR_ARGUMENT
+    # missing constants
+    bad = W.Network(W.NET_KATZ96, 5, 4)
+    assert _call(bad, np.ones((4, 5))) == _capi.WIND_ERR_ARGUMENT
+    # unknown network kind
+    bad = W.Network(99, 2, 4, constants=net.constants)
+    assert _call(bad, y) == _capi.WIND_ERR_ARGUMENT
+    # null state with systems to integrate
+    assert _call(net, None) == _capi.WIND_ERR_ARGUMENT
+    # bad memory flag
+    assert w.wind_integrate(C.byref(lib.options()), C.byref(ns), 0.0, 1.0, 1, y.ctypes.data, 4,
+                            1e-6, 1e-6, None, None, None, 5, None) == _capi.WIND_ERR_ARGUMENT
+    # n_integration_steps < 1
+    assert w.wind_integrate(C.byref(lib.options()), C.byref(ns), 0.0, 1.0, 0, y.ctypes.data, 4,
+                            1e-6, 1e-6, None, None, None, 0, None) == _capi.WIND_ERR_ARGUMENT
+
+
+def test_zero_systems_is_a_no_op():
+    net = W.nr_test(0)
+    assert _call(net, np.ones((0, 2))) == _capi.WIND_OK
+    w = lib.load()
+    assert w.wind_integrate_batch(C.byref(lib.options()), None, 0, None) == _capi.WIND_OK

@@ -1,0 +1,112 @@
+"""CPU tests of the oracle (test infrastructure): pinned against the golden
+vectors made by the reference's own CPU integrator, against the reference
+build itself when it is present, and against known answers."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as O
+from wind_b200 import networks as W
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = np.load(os.path.join(HERE, "golden", "golden.npz"))
+NAMES = sorted({k.split("/")[0] for k in GOLDEN.files})
+
+
+def golden_case(name):
+    meta = GOLDEN[f"{name}/meta"]
+    kind, n = int(meta[0]), int(meta[1])
+    arr = {k: GOLDEN[f"{name}/{k}"] for k in ("constants", "rates", "species", "linear")
+           if f"{name}/{k}" in GOLDEN.files}
+    y0 = GOLDEN[f"{name}/y0"]
+    net = W.Network(kind, n, y0.shape[0], **arr)
+    wl = W.Workload(net, y0, meta[2], meta[3], meta[4], meta[5], int(meta[6]), 1, name)
+    return wl, str(GOLDEN[f"{name}/method"]), GOLDEN[f"{name}/y"], int(meta[7])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_restatement_matches_golden(name):
+    """GOLD semantics reproduce the reference c_baseline bit for bit."""
+    wl, method, y_ref, tot_ref = golden_case(name)
+    y = wl.y0.copy()
+    tot, st, _ = O.restated(wl.net, y, wl.tnow, wl.tend, wl.atol, wl.rtol, method, "gold",
+                            wl.n_integration_steps)
+    assert np.array_equal(y, y_ref), f"max diff {np.max(np.abs(y - y_ref))}"
+    assert tot == tot_ref
+    assert st.max() == 0
+
+
+def _random_cases():
+    rng = np.random.default_rng(7)
+    k = W.workload_katz96(24, seed=9)
+    yield "katz96", "sie", W.Workload(k.net, k.y0, 0.0, 1e12, 1e-7, 1e-5, 1, 1)
+    yield "katz96", "rk2", W.Workload(k.net, k.y0, 0.0, 3e6, 1e-4, 1e-4, 1, 1)
+    nr = W.workload_nr(8, seed=5)
+    yield "nr", "sie", W.Workload(nr.net, nr.y0, 0.0, 0.003, 1e-8, 1e-6, 2, 1)
+    for n, r, lin in ((5, 50, False), (16, 160, False), (32, 64, True)):
+        net = W.random_mass_action(rng, 3, n, r, 1e-3, 1e1)
+        if lin:
+            net.linear = W.dense_linear(rng, 3, n, 1e-2, 1e4)
+        y0 = rng.uniform(0, 1, (3, n))
+        yield net.name, "sie", W.Workload(net, y0, 0.0, 1e-4, 1e-6, 1e-4, 1, 1)
+
+
+@pytest.mark.parametrize("case", list(_random_cases()), ids=lambda c: f"{c[0]}-{c[1]}")
+def test_restatement_matches_reference_build(case):
+    name, method, wl = case
+    if not O.reference_available(wl.net, method):
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    y_o, y_r = wl.y0.copy(), wl.y0.copy()
+    tot_o, _, _ = O.restated(wl.net, y_o, wl.tnow, wl.tend, wl.atol, wl.rtol, method, "gold",
+                             wl.n_integration_steps)
+    tot_r = O.reference(wl.net, y_r, wl.tnow, wl.tend, wl.atol, wl.rtol, method,
+                        wl.n_integration_steps)
+    assert np.array_equal(y_o, y_r)
+    assert tot_o == tot_r
+
+
+def test_nr_analytic_known_answer():
+    """NR test against its exact solution (python/ode_systems/NR_test.py:72-77
+    generalised to any initial condition) over t = 0..0.2 in 20 outputs."""
+    wl = W.workload_nr(8, seed=0)
+    y = wl.y0.copy()
+    t = 0.0
+    for _ in range(20):
+        O.restated(wl.net, y, t, t + 0.01, 1e-10, 1e-8, "rk2", "device")
+        t += 0.01
+    exact = W.nr_analytic(wl.y0, t)
+    assert np.max(np.abs(y - exact) / np.abs(exact)) < 1e-6
+
+
+def test_katz96_conserves_hydrogen():
+    """The H total y0+y1 is an invariant of the Katz96 RHS and the H block of
+    its Jacobian has zero column sums, so SIE conserves it to rounding.  (The
+    He total is not conserved by SIE: the reference Jacobian's J[13] = J[12]
+    (cuda/ode_system/ode_gold.c:79) breaks the zero column sum of the He
+    block; parity keeps that behaviour.)"""
+    wl = W.workload_katz96(64, seed=3)
+    y = wl.y0.copy()
+    O.restated(wl.net, y, 0.0, 1e12, 1e-8, 1e-6, "sie", "device", threads=4)
+    assert np.allclose(y[:, 0] + y[:, 1], 1.0, rtol=0, atol=1e-12)
+
+
+def test_oracle_edge_cases():
+    wl = W.workload_katz96(4, seed=1)
+    # empty range
+    y = wl.y0.copy()
+    tot, _, _ = O.restated(wl.net.subset(slice(0, 0)), y[:0], 0.0, 1.0, 1e-3, 1e-3)
+    assert tot == 0
+    # tnow == tend: nothing happens
+    y = wl.y0.copy()
+    tot, st, _ = O.restated(wl.net, y, 5.0, 5.0, 1e-3, 1e-3)
+    assert tot == 0 and np.array_equal(y, wl.y0)
+    # attempt budget
+    y = wl.y0.copy()
+    tot, st, n = O.restated(wl.net, y, 0.0, 1e13, 1e-10, 1e-10, max_attempts=3)
+    assert (n <= 9).all() and (st & 2).any()
+    # non-finite initial condition is reported, not trapped
+    y = wl.y0.copy()
+    y[1, 0] = np.nan
+    tot, st, _ = O.restated(wl.net, y, 0.0, 1e10, 1e-3, 1e-3)
+    assert st[1] & 1 and st[0] == 0
