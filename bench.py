@@ -43,13 +43,15 @@ METRIC = "systems/s at 1e-5 rel err vs FP64 (mixed vs plain FP64 GPU); serve p50
 
 
 # ---------------------------------------------------------------------------
-def make_workload(name: str):
+def make_workload(name: str, systems: int = 0):
     if name == "katz96":
-        wl = W.workload_katz96(65536, atol=1e-8, rtol=1e-6)
-        return wl, "Katz96 5-species, 65,536 cells, dt=1e13 s, atol=1e-8 rtol=1e-6"
+        n = systems or 65536
+        wl = W.workload_katz96(n, atol=1e-8, rtol=1e-6)
+        return wl, f"Katz96 5-species, {n:,} cells, dt=1e13 s, atol=1e-8 rtol=1e-6"
     if name == "katz96_loose":
-        wl = W.workload_katz96(65536)
-        return wl, "Katz96 5-species, 65,536 cells, dt=1e13 s, atol=rtol=5e-3"
+        n = systems or 65536
+        wl = W.workload_katz96(n)
+        return wl, f"Katz96 5-species, {n:,} cells, dt=1e13 s, atol=rtol=5e-3"
     if name == "nr":
         wl = W.workload_nr(1024)
         wl = W.Workload(wl.net, wl.y0, 0.0, 0.01, wl.atol, wl.rtol, 1, 1, "nr_test")
@@ -226,6 +228,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="wind", choices=["wind", "reference"])
     ap.add_argument("--workload", default="katz96")
+    ap.add_argument("--systems", type=int, default=0, help="override the system count "
+                    "(profiling runs on a small case; the headline uses the default)")
     ap.add_argument("--method", default="sie", choices=["sie", "rk2"])
     ap.add_argument("--solver", default="auto", choices=["auto", "gje_f64", "lu_f64", "mixed"])
     ap.add_argument("--spec-width", type=int, default=0)
@@ -234,7 +238,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    wl, desc = make_workload(args.workload)
+    wl, desc = make_workload(args.workload, args.systems)
     if args.impl == "reference":
         return run_reference_arm(args, wl, desc)
 

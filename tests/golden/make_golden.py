@@ -22,8 +22,29 @@ from oracle import pyoracle as O  # noqa: E402
 from wind_b200 import networks as W  # noqa: E402
 
 
+def reference_fixture(path="/root/reference/cuda/debug/inputKatz96_1_1_1.h"):
+    """The reference's committed debug input (4 Katz96 cells), parsed from the
+    header its dlopen driver includes (cuda/debug/debug.c:1); the driver runs
+    it with tend = 10 and abs = rel = 5e-3 (debug.c:19,29-30)."""
+    import re
+    src = open(path).read()
+
+    def arr(name):
+        m = re.search(name + r"\[\d+\]\s*=\s*\{([^}]*)\}", src)
+        return np.array([float(v) for v in m.group(1).split(",")], np.float32)
+
+    eq = arr("equations").astype(np.float64).reshape(4, 5)
+    c = arr("constants").astype(np.float64).reshape(4, 10)
+    net = W.Network(W.NET_KATZ96, 5, 4, constants=c)
+    return W.Workload(net, eq, 0.0, 10.0, float(np.float32(5e-3)), float(np.float32(5e-3)), 1, 1)
+
+
 def cases():
     out = []
+    if os.path.exists("/root/reference/cuda/debug/inputKatz96_1_1_1.h"):
+        fx = reference_fixture()
+        out.append(("fixture_katz96_debug_sie", "sie", fx))
+        out.append(("fixture_katz96_debug_rk2", "rk2", fx))
     nr = W.workload_nr(16, seed=100)
     out.append(("nr_sie", "sie", W.Workload(nr.net, nr.y0, 0.0, 0.01, 1e-8, 1e-6, 1, 1)))
     out.append(("nr_rk2", "rk2", W.Workload(nr.net, nr.y0, 0.0, 0.01, 1e-8, 1e-6, 1, 1)))

@@ -44,3 +44,18 @@ def mixed_err(a, b, atol):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), atol))) if a.size else 0.0
+
+
+def cta_workloads():
+    """Systems above 32 equations (the CTA-per-system kernels)."""
+    out = []
+    for n, dt in ((64, 1e-5), (157, 2e-6)):
+        w = W.workload_mixed(60, seed=31, sizes=(n,), fractions=(1.0,), dt=dt, atol=1e-6,
+                             rtol=1e-4)[0].subset(slice(0, 3))
+        out.append(W.Workload(w.net, w.y0, w.tnow, w.tend, w.atol, w.rtol, 1, 1, f"cta_n{n}"))
+    rng = np.random.default_rng(33)
+    net = W.random_mass_action(rng, 3, 40, 80, 1e-3, 1e1)
+    net.linear = W.dense_linear(rng, 3, 40, 1e-2, 1e4)
+    y0 = rng.uniform(0.0, 1.0, (3, 40))
+    out.append(W.Workload(net, y0, 0.0, 1e-4, 1e-6, 1e-4, 1, 1, "cta_n40_lin"))
+    return out

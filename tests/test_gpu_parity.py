@@ -83,3 +83,74 @@ def test_batch_matches_single_calls(cuda_device):
         y = wl.y0.copy()
         lib.integrate(wl.net, y, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", "gje_f64", "device")
         assert np.array_equal(yg, y)
+
+
+CTA = __import__("tests.helpers", fromlist=["cta_workloads"]).cta_workloads()
+
+
+@pytest.mark.parametrize("ctrl", ["gold", "device"])
+@pytest.mark.parametrize("wl", CTA, ids=_ids(CTA))
+def test_cta_gje_bitexact(cuda_device, wl, ctrl):
+    y_o = wl.y0.copy()
+    tot_o, st_o, n_o = O.restated(wl.net, y_o, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", ctrl,
+                                  threads=8)
+    y_g = wl.y0.copy()
+    tot_g, st_g, n_g = lib.integrate(wl.net, y_g, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie",
+                                     "gje_f64", ctrl)
+    assert np.array_equal(y_g, y_o), f"max diff {np.max(np.abs(y_g - y_o))}"
+    assert np.array_equal(n_g, n_o) and tot_g == tot_o
+
+
+@pytest.mark.parametrize("wl", CTA, ids=_ids(CTA))
+def test_cta_rk2_bitexact(cuda_device, wl):
+    wl = rk2_variant(wl)
+    y_o = wl.y0.copy()
+    tot_o, _, n_o = O.restated(wl.net, y_o, wl.tnow, wl.tend, wl.atol, wl.rtol, "rk2", "device")
+    y_g = wl.y0.copy()
+    tot_g, _, n_g = lib.integrate(wl.net, y_g, wl.tnow, wl.tend, wl.atol, wl.rtol, "rk2",
+                                  "gje_f64", "device")
+    assert np.array_equal(y_g, y_o) and tot_g == tot_o
+
+
+@pytest.mark.parametrize("solver", ["lu_f64", "mixed"])
+@pytest.mark.parametrize("wl", CTA, ids=_ids(CTA))
+def test_cta_fast_solvers_close(cuda_device, wl, solver):
+    y_o = wl.y0.copy()
+    O.restated(wl.net, y_o, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", "device", threads=8)
+    y_g = wl.y0.copy()
+    lib.integrate(wl.net, y_g, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", solver, "device")
+    assert mixed_err(y_g, y_o, wl.atol) <= 1e-5
+
+
+@pytest.mark.parametrize("nsys", [1, 3, 40, 5000])
+def test_lane_speculation_counts(cuda_device, nsys):
+    """Batch sizes from 1 to thousands exercise every team size of the
+    lane kernel's helpers; results must stay identical to the serial loop."""
+    wl = W.workload_katz96(nsys, seed=41, atol=1e-8, rtol=1e-6)
+    wl = W.Workload(wl.net, wl.y0, 0.0, 1e10, wl.atol, wl.rtol, 1, 1, "k")
+    y_o = wl.y0.copy()
+    tot_o, _, n_o = O.restated(wl.net, y_o, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", "device",
+                               threads=8)
+    y_g = wl.y0.copy()
+    tot_g, _, n_g = lib.integrate(wl.net, y_g, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie",
+                                  "gje_f64", "device")
+    assert np.array_equal(y_g, y_o) and np.array_equal(n_g, n_o)
+
+
+def test_bad_species_index_is_reported(cuda_device):
+    """A species index >= N is caught by the kernel's bounds check: the
+    system is flagged and left untouched, the others integrate normally."""
+    import torch
+    wl = [c for c in CASES if c.net.kind == W.NET_MASS_ACTION][0]
+    net = wl.net.subset(slice(0, 4))
+    sp = net.species.copy()
+    sp[2, 0, 1] = net.n_eq + 3
+    dev = torch.device("cuda", 0)
+    arrays = {"rates": torch.from_numpy(net.rates).to(dev),
+              "species": torch.from_numpy(sp).to(dev)}
+    y = torch.from_numpy(wl.y0[:4].copy()).to(dev)
+    _, status, _ = lib.integrate(net, y, wl.tnow, wl.tend, wl.atol, wl.rtol, device_arrays=arrays)
+    torch.cuda.synchronize()
+    st = status.cpu().numpy()
+    assert st[2] & 32 and (st[[0, 1, 3]] == 0).all()
+    assert np.array_equal(y.cpu().numpy()[2], wl.y0[2])

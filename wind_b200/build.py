@@ -27,7 +27,8 @@ FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                 "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 
 # translation units of libwind.so
-UNITS = ["api", "batch", "noalloc"]
+UNITS = ["api", "batch", "noalloc", "dispatch_lane", "dispatch_team", "dispatch_team8",
+         "dispatch_team16", "dispatch_team32", "dispatch_cta"]
 
 LEGACY_NETS = {"nr_test": "WIND_NET_NR_TEST", "katz96": "WIND_NET_KATZ96",
                "stifftrig": "WIND_NET_STIFFTRIG"}
@@ -61,15 +62,20 @@ def build_native(verbose=False):
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(OBJ, exist_ok=True)
     deps = _deps()
-    objs = []
+    objs, jobs = [], []
     for unit in UNITS:
         obj = os.path.join(OBJ, unit + ".o")
         objs.append(obj)
         if _stale(obj, deps):
             if verbose:
                 print(f"nvcc {unit}.cu", flush=True)
-            _run([NVCC] + FLAGS + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj],
-                 log=os.path.join(OBJ, unit + ".ptxas.log"))
+            jobs.append(([NVCC] + FLAGS + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj],
+                         os.path.join(OBJ, unit + ".ptxas.log")))
+    if jobs:
+        import concurrent.futures as cf
+        with cf.ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+            for f in [ex.submit(_run, cmd, log) for cmd, log in jobs]:
+                f.result()
     libwind = os.path.join(LIB, "libwind.so")
     if _stale(libwind, objs):
         _run([NVCC] + ARCH + ["-shared"] + objs + ["-o", libwind, "-lcudart"])

@@ -15,8 +15,7 @@
 #include <vector>
 
 #include "api_internal.h"
-#include "lane_kernel.cuh"
-#include "team_kernel.cuh"
+#include "networks.cuh"
 
 using namespace wind;
 
@@ -41,35 +40,6 @@ static int builtin_nc(int kind) {
     }
 }
 
-// ---- lane kernel dispatch ------------------------------------------------
-using LaneFn = void (*)(KParams, int);
-
-template <class Net, int METHOD, int CTRL>
-static LaneFn lane_by_solver(int solver) {
-    if (METHOD == WIND_METHOD_RK2) return k_lane<Net, METHOD, CTRL, 0>;
-    switch (solver) {
-    case WIND_SOLVER_GJE_F64: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_GJE_F64>;
-    case WIND_SOLVER_LU_F64: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_LU_F64>;
-    default: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_MIXED>;
-    }
-}
-template <class Net>
-static LaneFn lane_for_net(int method, int ctrl, int solver) {
-    if (method == WIND_METHOD_SIE)
-        return ctrl == WIND_CTRL_GOLD ? lane_by_solver<Net, WIND_METHOD_SIE, WIND_CTRL_GOLD>(solver)
-                                      : lane_by_solver<Net, WIND_METHOD_SIE, WIND_CTRL_DEVICE>(solver);
-    return ctrl == WIND_CTRL_GOLD ? lane_by_solver<Net, WIND_METHOD_RK2, WIND_CTRL_GOLD>(solver)
-                                  : lane_by_solver<Net, WIND_METHOD_RK2, WIND_CTRL_DEVICE>(solver);
-}
-static LaneFn lane_kernel(int kind, int method, int ctrl, int solver) {
-    switch (kind) {
-    case WIND_NET_NR_TEST: return lane_for_net<NetNR>(method, ctrl, solver);
-    case WIND_NET_KATZ96: return lane_for_net<NetKatz96>(method, ctrl, solver);
-    case WIND_NET_STIFFTRIG: return lane_for_net<NetTrig>(method, ctrl, solver);
-    default: return nullptr;
-    }
-}
-
 int device_sm_count() {
     int dev = 0, n = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 148;
@@ -77,31 +47,11 @@ int device_sm_count() {
     return n;
 }
 
-static int lane_blocks_per_sm(LaneFn fn) {
-    static std::mutex mu;
-    static std::vector<std::pair<const void*, int>> cache;
-    std::lock_guard<std::mutex> g(mu);
-    for (auto& e : cache)
-        if (e.first == (const void*)fn) return e.second;
-    int nb = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, LANE_THREADS, 0) != cudaSuccess || nb < 1)
-        nb = 1;
-    cache.push_back({(const void*)fn, nb});
-    return nb;
-}
-
-int choose_width(int64_t nsys, int slots, int method, int ctrl) {
-    const int cap = (ctrl == WIND_CTRL_DEVICE && method == WIND_METHOD_RK2) ? 20 : 10;
-    const int wmax = cap >= 16 ? 32 : 16;
-    int w = 1;
-    while (w < wmax && nsys * (int64_t)(2 * w) <= (int64_t)slots) w *= 2;
-    return w;
-}
-
 wind_status check_network(const wind_network* net, int64_t nsys) {
     if (!net) return WIND_ERR_ARGUMENT;
     if (net->kind == WIND_NET_MASS_ACTION) {
-        if (net->n_eq < 1 || net->n_eq > TEAM_MAXN) return WIND_ERR_UNSUPPORTED;
+        if (net->n_eq < 1 || net->n_eq > WIND_MAX_EQ) return WIND_ERR_UNSUPPORTED;
+        if (net->n_react > 65535) return WIND_ERR_UNSUPPORTED;
         if (net->n_react < 0) return WIND_ERR_ARGUMENT;
         if (nsys > 0 && net->n_react > 0 && (!net->rates || !net->species)) return WIND_ERR_ARGUMENT;
         return WIND_OK;
@@ -116,23 +66,21 @@ wind_status check_network(const wind_network* net, int64_t nsys) {
 
 // Launch the right kernel family for one homogeneous batch already on the
 // device.  `p.counters` must point at zeroed device counters.
-wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream_t stream) {
+wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream_t stream,
+                             bool allow_alloc) {
     if (p.nsys == 0) return WIND_OK;
-    if (p.kind != WIND_NET_MASS_ACTION) {
-        LaneFn fn = lane_kernel(p.kind, o.method, o.controller, o.solver);
-        if (!fn) return WIND_ERR_UNSUPPORTED;
-        const int nb = lane_blocks_per_sm(fn);
-        const int slots = nb * device_sm_count() * LANE_THREADS;
-        int w = o.spec_width;
-        if (w <= 0) w = choose_width(p.nsys, slots, o.method, o.controller);
-        if (w != 1 && w != 2 && w != 4 && w != 8 && w != 16 && w != 32) return WIND_ERR_ARGUMENT;
-        const int64_t need = (p.nsys * w + LANE_THREADS - 1) / LANE_THREADS;
-        const int grid = (int)(need < (int64_t)nb * device_sm_count() ? need : (int64_t)nb * device_sm_count());
-        fn<<<grid, LANE_THREADS, 0, stream>>>(p, w);
-        g_launches++;
-        return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
-    }
-    return launch_team(o, p, stream);
+    if (p.kind != WIND_NET_MASS_ACTION) return launch_lane(o, p, stream);
+    if (p.n_eq <= WIND_TEAM_MAX_EQ) return launch_team(o, p, stream);
+    // CTA kernels: global scratch for the matrices that do not fit in shared
+    // memory, taken from the stream-ordered pool and returned after the launch
+    const size_t need = cta_scratch_bytes(o, p, nullptr);
+    if (need == 0) return launch_cta(o, p, stream, nullptr, 0);
+    if (!allow_alloc) return WIND_ERR_UNSUPPORTED;
+    double* scratch = nullptr;
+    if (cudaMallocAsync((void**)&scratch, need, stream) != cudaSuccess) return WIND_ERR_NOMEM;
+    const wind_status st = launch_cta(o, p, stream, scratch, need);
+    cudaFreeAsync(scratch, stream);
+    return st;
 }
 
 }  // namespace wind
@@ -196,70 +144,6 @@ int wind_integrate(const wind_options* opt_in, const wind_network* net, double t
 }
 
 }  // extern "C"
-
-// ---- team kernel dispatch (mass action, N <= 32) ---------------------------
-namespace wind {
-
-using TeamFn = void (*)(KParams);
-
-template <int NMAX, int METHOD, int CTRL>
-static TeamFn team_by_solver(int solver) {
-    if (METHOD == WIND_METHOD_RK2) return k_team<NMAX, METHOD, CTRL, 0>;
-    switch (solver) {
-    case WIND_SOLVER_GJE_F64: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_GJE_F64>;
-    case WIND_SOLVER_LU_F64: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_LU_F64>;
-    default: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_MIXED>;
-    }
-}
-template <int NMAX>
-static TeamFn team_for_nmax(int method, int ctrl, int solver) {
-    if (method == WIND_METHOD_SIE)
-        return ctrl == WIND_CTRL_GOLD ? team_by_solver<NMAX, WIND_METHOD_SIE, WIND_CTRL_GOLD>(solver)
-                                      : team_by_solver<NMAX, WIND_METHOD_SIE, WIND_CTRL_DEVICE>(solver);
-    return ctrl == WIND_CTRL_GOLD ? team_by_solver<NMAX, WIND_METHOD_RK2, WIND_CTRL_GOLD>(solver)
-                                  : team_by_solver<NMAX, WIND_METHOD_RK2, WIND_CTRL_DEVICE>(solver);
-}
-
-int team_nmax(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : 32); }
-
-size_t team_smem_bytes(int n, int R, bool lin) {
-    const int nmax = team_nmax(n);
-    return (size_t)(TEAM_THREADS / nmax) * TeamLayout(nmax, R, lin).bytes;
-}
-
-static int team_blocks_per_sm(TeamFn fn, size_t smem) {
-    static std::mutex mu;
-    static std::vector<std::pair<std::pair<const void*, size_t>, int>> cache;
-    std::lock_guard<std::mutex> g(mu);
-    for (auto& e : cache)
-        if (e.first.first == (const void*)fn && e.first.second == smem) return e.second;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int nb = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, TEAM_THREADS, smem) != cudaSuccess || nb < 1)
-        nb = 0;
-    cache.push_back({{(const void*)fn, smem}, nb});
-    return nb;
-}
-
-wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream) {
-    const int nmax = team_nmax(p.n_eq);
-    TeamFn fn = nmax == 8 ? team_for_nmax<8>(o.method, o.controller, o.solver)
-              : nmax == 16 ? team_for_nmax<16>(o.method, o.controller, o.solver)
-                           : team_for_nmax<32>(o.method, o.controller, o.solver);
-    const size_t smem = team_smem_bytes(p.n_eq, p.n_react, p.linear != nullptr);
-    if (smem > 227 * 1024) return WIND_ERR_UNSUPPORTED;
-    const int nb = team_blocks_per_sm(fn, smem);
-    if (nb < 1) return WIND_ERR_UNSUPPORTED;
-    const int teams = TEAM_THREADS / nmax;
-    const int64_t need = (p.nsys + teams - 1) / teams;
-    const int64_t cap = (int64_t)nb * device_sm_count();
-    const int grid = (int)(need < cap ? need : cap);
-    fn<<<grid, TEAM_THREADS, smem, stream>>>(p);
-    g_launches++;
-    return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
-}
-
-}  // namespace wind
 
 // ---- device-resident output loop and multi-group batch ---------------------
 extern "C" {

@@ -1,6 +1,7 @@
 // api_internal.h -- host-side pieces shared by the entry points.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -11,8 +12,21 @@ namespace wind {
 
 int device_sm_count();
 wind_status check_network(const wind_network* net, int64_t nsys);
-wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream_t stream);
+// Launch the kernel family for one homogeneous batch.  `allow_alloc` = false
+// makes configurations that need global scratch return WIND_ERR_UNSUPPORTED
+// instead of taking it from the stream-ordered allocator.
+wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream_t stream,
+                             bool allow_alloc = true);
 wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream);
+wind_status launch_lane(const wind_options& o, const KParams& p, cudaStream_t stream);
+size_t cta_scratch_bytes(const wind_options& o, const KParams& p, int* grid_out);
+wind_status launch_cta(const wind_options& o, const KParams& p, cudaStream_t stream, double* scratch,
+                       size_t scratch_bytes);
+extern std::atomic<int64_t> g_launches;
+// Largest N any kernel family accepts (lane/team kernels up to 32, CTA
+// kernels up to 256).
+constexpr int WIND_MAX_EQ = 256;
+constexpr int WIND_TEAM_MAX_EQ = 32;
 
 // One wind_integrate call: device copies of host inputs (when memory is
 // HOST), the counters block, and the kernel parameters.  Allocations are

@@ -67,6 +67,27 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 __device__ __forceinline__ bool finite64(double x) { return isfinite(x); }
 
+// Reciprocals for the LU and mixed solvers (not bit-exact by design): the
+// hardware approximation refined by Newton-Raphson, y <- y + y(1 - b y)
+// (Muller et al., Handbook of Floating-Point Arithmetic, 2nd ed., sec. 4.7 /
+// 5.3); each step doubles the correct bits.  Stays inline, so the solvers
+// need no call frame.  b = 0 gives NaN (a singular pivot).
+__device__ __forceinline__ double nr_rcp(double b) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    double e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    return y;
+}
+__device__ __forceinline__ float nr_rcp(float b) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+    const float e = fmaf(-b, y, 1.0f);
+    return fmaf(y, e, y);
+}
+
 // Refinement cap before an attempt is accepted regardless of its error:
 // kernel.cu:259 (RK2 20, SIE 10) for DEVICE, common_gold.c:121 (10) for GOLD.
 template <int METHOD, int CTRL>

@@ -1,0 +1,56 @@
+// dispatch_team.cu -- launch of the team-per-system kernels (mass action,
+// N <= 32).
+#include <mutex>
+#include <vector>
+
+#include "api_internal.h"
+#include "team_kernel.cuh"
+
+namespace wind {
+
+using TeamFn = void (*)(KParams);
+TeamFn team_fn_8(int method, int ctrl, int solver);
+TeamFn team_fn_16(int method, int ctrl, int solver);
+TeamFn team_fn_32(int method, int ctrl, int solver);
+
+int team_nmax(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : 32); }
+
+size_t team_smem_bytes(int n, int R, bool lin) {
+    const int nmax = team_nmax(n);
+    return (size_t)(TEAM_THREADS / nmax) * TeamLayout(nmax, R, lin).bytes;
+}
+
+static int team_blocks_per_sm(TeamFn fn, size_t smem) {
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const void*, size_t>, int>> cache;
+    std::lock_guard<std::mutex> g(mu);
+    for (auto& e : cache)
+        if (e.first.first == (const void*)fn && e.first.second == smem) return e.second;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, TEAM_THREADS, smem) != cudaSuccess || nb < 1)
+        nb = 0;
+    cache.push_back({{(const void*)fn, smem}, nb});
+    return nb;
+}
+
+wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream) {
+    const int nmax = team_nmax(p.n_eq);
+    TeamFn fn = nmax == 8 ? team_fn_8(o.method, o.controller, o.solver)
+              : nmax == 16 ? team_fn_16(o.method, o.controller, o.solver)
+                           : team_fn_32(o.method, o.controller, o.solver);
+    const size_t smem = team_smem_bytes(p.n_eq, p.n_react, p.linear != nullptr);
+    if (smem > 227 * 1024) return WIND_ERR_UNSUPPORTED;
+    const int nb = team_blocks_per_sm(fn, smem);
+    if (nb < 1) return WIND_ERR_UNSUPPORTED;
+    const int teams = TEAM_THREADS / nmax;
+    const int64_t need = (p.nsys + teams - 1) / teams;
+    const int64_t cap = (int64_t)nb * device_sm_count();
+    const int grid = (int)(need < cap ? need : cap);
+    fn<<<grid, TEAM_THREADS, smem, stream>>>(p);
+    g_launches++;
+    return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
+}
+
+}  // namespace wind
+

@@ -128,7 +128,9 @@ template <class Net, int METHOD, int CTRL, int SOLVER>
 __device__ __forceinline__ void lane_take_step(const double (&c)[Net::NC], double t0, double H,
                                                int nsub, xd (&y)[Net::N]) {
     const double t1 = t0 + H;
-    double h = (t1 - t0) / nsub;
+    // (t1-t0)/nsub for nsub in {1,2}: multiplying by 1 or 0.5 rounds the
+    // same real number, so it equals the division bit for bit
+    double h = (t1 - t0) * (nsub == 1 ? 1.0 : 0.5);
     double t = t0;
     for (int i = 0; i < nsub; i++) {
         if (CTRL == WIND_CTRL_DEVICE) h = fmin(t1 - t, h);
@@ -137,93 +139,182 @@ __device__ __forceinline__ void lane_take_step(const double (&c)[Net::NC], doubl
     }
 }
 
+// Lanes of the warp that point at the same owner form a team.  With a
+// systems in the warp (owners), lane i works on owner (i mod a) at
+// refinement level (i div a): lanes are spread round-robin, so team sizes
+// differ by at most one and the lowest lane of a team carries level 0.
+__device__ __forceinline__ unsigned team_mask_of(int j, int nact, int wmax) {
+    unsigned m = 0u;
+    for (int k = j, r = 0; k < 32 && r < wmax; k += nact, r++) m |= 1u << k;
+    return m;
+}
+
+// Persistent kernel.  Every lane owns at most one system (its state lives in
+// the owner's registers).  Each round:
+//  1. lanes without a system take the next ticket from the work queue;
+//  2. the a owned systems of the warp are assigned all 32 lanes round-robin;
+//     a lane fetches its assigned system's state from the owner by shuffle;
+//  3. each lane evaluates one attempt (full step + two half steps + error
+//     test) at its refinement level;
+//  4. per team, the lowest level that passes (or the one at the cap) is the
+//     accepted attempt; every level below it is exactly the serial
+//     controller's rejected attempt, so the owner applies "levels refined,
+//     then accept" with results identical to the serial loop.
+// While the queue is full every lane owns a system and a round is one attempt
+// per system (no speculation, no waste).  As the queue drains, idle lanes join
+// the remaining systems, which cuts the tail of slow systems by up to the
+// refinement cap.  Only lanes below `opw` (owners per warp) take tickets; the
+// others start as helpers, which spreads a small batch over many warps
+// (opw = 32 / initial lanes per system).
 template <class Net, int METHOD, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(LANE_THREADS) k_lane(const KParams p, const int W) {
+__global__ void __launch_bounds__(LANE_THREADS) k_lane(const KParams p, const int opw) {
     constexpr int N = Net::N;
     constexpr int NC = Net::NC;
     constexpr int CAP = Cap<METHOD, CTRL>::value;
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int wmax = 32;
     const int lane = threadIdx.x & 31;
-    const int level = lane % W;
-    const int leader = lane - level;
-    const unsigned team_mask = (W >= 32) ? 0xffffffffu : (((1u << W) - 1u) << leader);
     const uint64_t t_start = p.timeout_ns ? global_ns() : 0;
+    const double tend = p.tend;
+
+    // owner state
+    bool has = false, drained = (lane >= opw);
+    int64_t s_own = -1;
+    double y_own[N];
+    double t_own = 0.0, h_own = 0.0;
+    int u_own = 0;
+    int64_t a_own = 0;
+    int32_t st_own = WIND_SYS_OK;
+    // worker cache
+    int64_t s_work = -1;
+    double c[NC];
 
     while (true) {
-        unsigned long long ticket = 0;
-        if (level == 0) ticket = atomicAdd(&p.counters[CNT_QUEUE], 1ull);
-        ticket = __shfl_sync(team_mask, ticket, leader);
-        const int64_t s = (int64_t)ticket;
-        if (s >= p.nsys) break;
-
-        double c[NC];
+        // 1. refill: take new tickets while without a system
+        while (!has && !drained) {
+            const unsigned long long ticket = atomicAdd(&p.counters[CNT_QUEUE], 1ull);
+            if ((int64_t)ticket >= p.nsys) { drained = true; break; }
+            s_own = (int64_t)ticket;
 #pragma unroll
-        for (int k = 0; k < NC; k++) c[k] = __ldg(p.constants + s * p.n_const + k);
+            for (int i = 0; i < N; i++) y_own[i] = p.y[s_own * N + i];
+            t_own = p.tnow;
+            h_own = p.h0;
+            u_own = 0;
+            a_own = 0;
+            st_own = WIND_SYS_OK;
+            has = true;
+        }
+        // finish systems that are done
+        if (has) {
+            bool fin = !(t_own < tend);
+            if (!fin && a_own >= p.max_attempts) { st_own |= WIND_SYS_MAX_ATTEMPTS; fin = true; }
+            if (!fin && p.timeout_ns && global_ns() - t_start > p.timeout_ns) {
+                st_own |= WIND_SYS_TIMEOUT;
+                fin = true;
+            }
+            if (fin) {
+#pragma unroll
+                for (int i = 0; i < N; i++) {
+                    if (!finite64(y_own[i])) st_own |= WIND_SYS_NONFINITE;
+                    p.y[s_own * N + i] = y_own[i];
+                }
+                if (p.sys_status) p.sys_status[s_own] = st_own;
+                if (p.sys_nsteps) p.sys_nsteps[s_own] = 3 * a_own;
+                atomicAdd(&p.counters[CNT_STEPS], (unsigned long long)(3 * a_own));
+                has = false;
+                continue;  // refill before the warp-wide round
+            }
+        }
+        const unsigned owners = __ballot_sync(FULL, has);
+        if (owners == 0u) {
+            if (__all_sync(FULL, drained)) break;
+            continue;
+        }
+        // 2. assignment and state fetch
+        const int nact = __popc(owners);
+        const int j = lane % nact;
+        const int r = lane / nact;
+        const int src = __fns(owners, 0, j + 1);
+        const int64_t s_j = __shfl_sync(FULL, s_own, src);
+        const double t_j = __shfl_sync(FULL, t_own, src);
+        const double h_j = __shfl_sync(FULL, h_own, src);
+        const int u_j = __shfl_sync(FULL, u_own, src);
+        const int64_t a_j = __shfl_sync(FULL, a_own, src);
         xd y[N];
 #pragma unroll
-        for (int i = 0; i < N; i++) y[i] = p.y[s * N + i];
-
-        double tnow = p.tnow;
-        const double tend = p.tend;
-        double h = p.h0;
-        int unsolved = 0;
-        int64_t attempts = 0;
-        int32_t st = WIND_SYS_OK;
-        while (tnow < tend) {
-            if (attempts >= p.max_attempts) { st |= WIND_SYS_MAX_ATTEMPTS; break; }
-            if (p.timeout_ns && global_ns() - t_start > p.timeout_ns) { st |= WIND_SYS_TIMEOUT; break; }
-            // kernel.cu:195 / common_gold.c:79
-            const double hw = fmin(tend - tnow, h);
-            double hl = hw;
-            for (int q = 0; q < level; q++) hl /= 2.0;
-            const int lvl = unsolved + level;
-            const bool valid = (lvl <= CAP) && (attempts + level < p.max_attempts);
-            xd y1[N], y2[N];
+        for (int i = 0; i < N; i++) y[i] = __shfl_sync(FULL, y_own[i], src);
+        if (s_j != s_work) {
+            s_work = s_j;
 #pragma unroll
-            for (int i = 0; i < N; i++) { y1[i] = y[i]; y2[i] = y[i]; }
-            bool err = true;
-            if (valid) {
-                lane_take_step<Net, METHOD, CTRL, SOLVER>(c, tnow, hl, 1, y1);
-                lane_take_step<Net, METHOD, CTRL, SOLVER>(c, tnow, hl, 2, y2);
-                err = false;
-#pragma unroll
-                for (int i = 0; i < N; i++) err |= elem_error<METHOD, CTRL>(y1[i], y2[i], p.atol, p.rtol);
-            }
-            const bool acc = valid && (!err || lvl == CAP);
-            const unsigned bal = __ballot_sync(team_mask, acc);
-            if (bal == 0) {
-                // every evaluated level refines: kernel.cu:259-270
-                int done = W;
-                if (attempts + W > p.max_attempts) done = (int)(p.max_attempts - attempts);
-                attempts += done;
-                unsolved += done;
-                h = hw;
-                for (int q = 0; q < done; q++) h /= 2.0;
-                continue;
-            }
-            const int a_lane = __ffs(bal) - 1;
-            attempts += (a_lane - leader) + 1;
-            double ynew[N];
-#pragma unroll
-            for (int i = 0; i < N; i++)
-                ynew[i] = (METHOD == WIND_METHOD_RK2) ? (xd(2.0) * y2[i] - y1[i]).v : y2[i].v;
-            const double ha = __shfl_sync(team_mask, hl, a_lane);
-#pragma unroll
-            for (int i = 0; i < N; i++) y[i] = __shfl_sync(team_mask, ynew[i], a_lane);
-            unsolved = 0;
-            if (tnow + ha == tnow) { st |= WIND_SYS_STALLED; break; }
-            tnow += ha;
-            // kernel.cu:271-294: RK2 doubles h, SIE goes for gold
-            h = (METHOD == WIND_METHOD_RK2) ? ha * 2 : tend - tnow;
+            for (int k = 0; k < NC; k++) c[k] = __ldg(p.constants + s_j * p.n_const + k);
         }
+        // 3. one attempt at level r: kernel.cu:195 / common_gold.c:79 clamp,
+        //    then r halvings (kernel.cu:262 / common_gold.c:123)
+        const double hw = fmin(tend - t_j, h_j);
+        double hl = hw;
+        for (int q = 0; q < r; q++) hl /= 2.0;
+        const int lvl = u_j + r;
+        const bool valid = (r < wmax) && (lvl <= CAP) && (a_j + r < p.max_attempts);
+        xd y1[N], y2[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) { y1[i] = y[i]; y2[i] = y[i]; }
+        bool err = true;
+        if (valid) {
+            lane_take_step<Net, METHOD, CTRL, SOLVER>(c, t_j, hl, 1, y1);
+            lane_take_step<Net, METHOD, CTRL, SOLVER>(c, t_j, hl, 2, y2);
+            err = false;
+#pragma unroll
+            for (int i = 0; i < N; i++) err |= elem_error<METHOD, CTRL>(y1[i], y2[i], p.atol, p.rtol);
+        }
+        const bool acc = valid && (!err || lvl == CAP);
+        const unsigned bal = __ballot_sync(FULL, acc);
+        // 4. owners apply their team's outcome
+        int take = lane;   // lane whose attempt this owner adopts (self = none)
+        int done = 0;      // attempts consumed this round
+        bool accepted = false;
+        if (has) {
+            const int jo = __popc(owners & ((1u << lane) - 1u));
+            const unsigned tm = team_mask_of(jo, nact, wmax);
+            const int tsz = __popc(tm);
+            const unsigned mine = bal & tm;
+            if (mine) {
+                take = __ffs(mine) - 1;
+                done = take / nact + 1;
+                accepted = true;
+            } else {
+                // every level of the team refined (the cap level would accept)
+                int lim = tsz;
+                if (a_own + lim > p.max_attempts) lim = (int)(p.max_attempts - a_own);
+                done = lim;
+            }
+        }
+        double ytake[N];
 #pragma unroll
         for (int i = 0; i < N; i++)
-            if (!finite64(y[i].v)) st |= WIND_SYS_NONFINITE;
-        if (level == 0) {
+            ytake[i] = (METHOD == WIND_METHOD_RK2) ? (xd(2.0) * y2[i] - y1[i]).v : y2[i].v;
+        const double htake = __shfl_sync(FULL, hl, take);
 #pragma unroll
-            for (int i = 0; i < N; i++) p.y[s * N + i] = y[i].v;
-            if (p.sys_status) p.sys_status[s] = st;
-            if (p.sys_nsteps) p.sys_nsteps[s] = 3 * attempts;
-            atomicAdd(&p.counters[CNT_STEPS], (unsigned long long)(3 * attempts));
+        for (int i = 0; i < N; i++) ytake[i] = __shfl_sync(FULL, ytake[i], take);
+        if (has) {
+            a_own += done;
+            if (accepted) {
+#pragma unroll
+                for (int i = 0; i < N; i++) y_own[i] = ytake[i];
+                u_own = 0;
+                if (t_own + htake == t_own) {
+                    st_own |= WIND_SYS_STALLED;
+                    t_own = tend;  // finishes at the top of the next round
+                } else {
+                    t_own += htake;
+                    // kernel.cu:285-294: RK2 doubles h, SIE goes for gold
+                    h_own = (METHOD == WIND_METHOD_RK2) ? htake * 2 : tend - t_own;
+                }
+            } else {
+                u_own += done;
+                double hh = fmin(tend - t_own, h_own);
+                for (int q = 0; q < done; q++) hh /= 2.0;
+                h_own = hh;
+            }
         }
     }
 }

@@ -26,7 +26,10 @@
 //    device current, on the first call made on it; make that first call
 //    before any stream capture on the device;
 //  * the groups run one after another on the caller's stream (no streams or
-//    events are created).
+//    events are created);
+//  * groups whose kernels need matrix scratch in global memory (mass-action
+//    networks with N > 32 whose factor does not fit in shared memory, and the
+//    Gauss-Jordan solver for N > 32) return WIND_ERR_UNSUPPORTED.
 #include <mutex>
 
 #include "api_internal.h"
@@ -102,7 +105,7 @@ extern "C" int wind_integrate_batch_noalloc(const wind_options* opt_in, const wi
         p.counters = scratch + (size_t)g * wind::CNT_SLOTS;
         p.max_attempts = o.max_attempts > 0 ? o.max_attempts : ((int64_t)1 << 40);
         p.timeout_ns = o.timeout_s > 0 ? (uint64_t)(o.timeout_s * 1e9) : 0;
-        st = wind::launch_integrate(o, p, stream);
+        st = wind::launch_integrate(o, p, stream, /*allow_alloc=*/false);
     }
     return st;
 }

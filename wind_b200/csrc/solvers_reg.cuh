@@ -80,7 +80,7 @@ __device__ __forceinline__ void lu_factor_reg(T (&A)[N * N], T (&rinv)[N], int (
             perm[i] = sw ? pb : pa;
             perm[k] = sw ? pa : pb;
         }
-        T r = T(1) / A[i * N + i];
+        T r = nr_rcp(A[i * N + i]);
         rinv[i] = r;
 #pragma unroll
         for (int k = i + 1; k < N; k++) {

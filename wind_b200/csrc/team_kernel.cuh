@@ -233,7 +233,7 @@ struct TeamLU {
                 double* buf = c.bc + (i & 1) * (2 * NMAX + 4);
                 if (l == p) {
                     mystep = i;
-                    rinv = (T)1 / Ar[i];
+                    rinv = nr_rcp(Ar[i]);
 #pragma unroll
                     for (int t = 0; t < NMAX; t++) buf[t] = (double)Ar[t];
                     buf[2 * NMAX] = (double)rinv;
@@ -326,7 +326,9 @@ template <int NMAX, int METHOD, int CTRL, int SOLVER>
 __device__ __forceinline__ void team_take_step(const TeamCtx<NMAX>& c, double t0, double H,
                                                int nsub) {
     const double t1 = t0 + H;
-    double h = (t1 - t0) / nsub;
+    // (t1-t0)/nsub for nsub in {1,2}: multiplying by 1 or 0.5 rounds the
+    // same real number, so it equals the division bit for bit
+    double h = (t1 - t0) * (nsub == 1 ? 1.0 : 0.5);
     double t = t0;
     for (int i = 0; i < nsub; i++) {
         if (CTRL == WIND_CTRL_DEVICE) h = fmin(t1 - t, h);
