@@ -141,7 +141,7 @@ def test_bad_species_index_is_reported(cuda_device):
     """A species index >= N is caught by the kernel's bounds check: the
     system is flagged and left untouched, the others integrate normally."""
     import torch
-    wl = [c for c in CASES if c.net.kind == W.NET_MASS_ACTION][0]
+    wl = [c for c in CASES if c.net.kind == W.NET_MASS_ACTION and c.net.linear is None][0]
     net = wl.net.subset(slice(0, 4))
     sp = net.species.copy()
     sp[2, 0, 1] = net.n_eq + 3

@@ -28,6 +28,17 @@ extern std::atomic<int64_t> g_launches;
 constexpr int WIND_MAX_EQ = 256;
 constexpr int WIND_TEAM_MAX_EQ = 32;
 
+// True for null or for memory a kernel may dereference (device or managed).
+inline bool device_ptr(const void* ptr) {
+    if (!ptr) return true;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();  // clear the error of an unknown pointer
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 // One wind_integrate call: device copies of host inputs (when memory is
 // HOST), the counters block, and the kernel parameters.  Allocations are
 // stream-ordered (cudaMallocAsync / cudaFreeAsync) and released in release().
@@ -86,6 +97,12 @@ struct IntegrateCall {
         if (cudaMemsetAsync(p.counters, 0, CNT_SLOTS * sizeof(unsigned long long), stream) != cudaSuccess)
             return WIND_ERR_CUDA;
         if (mem == WIND_MEM_DEVICE) {
+            // every array must be device (or managed) memory of a device:
+            // a host pointer handed to a kernel would fault
+            if (!device_ptr(net.constants) || !device_ptr(net.rates) || !device_ptr(net.species) ||
+                !device_ptr(net.linear) || !device_ptr(y) || !device_ptr(sys_status) ||
+                !device_ptr(sys_nsteps))
+                return WIND_ERR_ARGUMENT;
             p.constants = net.constants;
             p.rates = net.rates;
             p.species = net.species;

@@ -14,6 +14,12 @@ wind_status launch_batch(const wind_options& o, const wind_group* groups, int ng
         if (st != WIND_OK) return st;
         if (groups[g].nsys > 0 && !groups[g].y) return WIND_ERR_ARGUMENT;
         if (groups[g].n_integration_steps < 1) return WIND_ERR_ARGUMENT;
+        const wind_network& gn = groups[g].net;
+        if (!wind::device_ptr(gn.constants) || !wind::device_ptr(gn.rates) ||
+            !wind::device_ptr(gn.species) || !wind::device_ptr(gn.linear) ||
+            !wind::device_ptr(groups[g].y) || !wind::device_ptr(groups[g].sys_status) ||
+            !wind::device_ptr(groups[g].sys_nsteps))
+            return WIND_ERR_ARGUMENT;
     }
     if (ngroups == 0) return WIND_OK;
     unsigned long long* counters = nullptr;

@@ -73,6 +73,12 @@ extern "C" int wind_integrate_batch_noalloc(const wind_options* opt_in, const wi
         if (st != WIND_OK) return st;
         if (groups[g].nsys > 0 && !groups[g].y) return WIND_ERR_ARGUMENT;
         if (groups[g].n_integration_steps < 1) return WIND_ERR_ARGUMENT;
+        const wind_network& gn = groups[g].net;
+        if (!wind::device_ptr(gn.constants) || !wind::device_ptr(gn.rates) ||
+            !wind::device_ptr(gn.species) || !wind::device_ptr(gn.linear) ||
+            !wind::device_ptr(groups[g].y) || !wind::device_ptr(groups[g].sys_status) ||
+            !wind::device_ptr(groups[g].sys_nsteps))
+            return WIND_ERR_ARGUMENT;
     }
     if (ngroups == 0) return WIND_OK;
     cudaStream_t stream = (cudaStream_t)stream_v;

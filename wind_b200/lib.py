@@ -96,7 +96,13 @@ def integrate(net: Network, y, tnow: float, tend: float, atol: float, rtol: floa
     if _is_torch(y):
         import torch
         assert y.dtype == torch.float64 and y.is_contiguous()
-        ns = _capi.network_struct(net, device_arrays or {})
+        device_arrays = device_arrays or {}
+        for k in ("constants", "rates", "species", "linear"):
+            if getattr(net, k) is not None:
+                a = device_arrays.get(k)
+                if a is None or not getattr(a, "is_cuda", False):
+                    raise ValueError(f"device call: network array '{k}' must be a CUDA tensor")
+        ns = _capi.network_struct(net, device_arrays)
         status = torch.zeros(net.nsys, dtype=torch.int32, device=y.device) if want_status else None
         nsteps = torch.zeros(net.nsys, dtype=torch.int64, device=y.device) if want_status else None
         code = lib.wind_integrate(C.byref(o), C.byref(ns), tnow, tend, n_integration_steps,
