@@ -154,3 +154,22 @@ def test_bad_species_index_is_reported(cuda_device):
     st = status.cpu().numpy()
     assert st[2] & 32 and (st[[0, 1, 3]] == 0).all()
     assert np.array_equal(y.cpu().numpy()[2], wl.y0[2])
+
+
+@pytest.mark.parametrize("solver", ["gje_f64", "lu_f64", "mixed"])
+def test_mixed_size_single_launch(cuda_device, solver):
+    """Mass-action groups of N = 5, 16, 32, 40, 64 (plus a builtin group) in
+    one wind_integrate_batch call: the mass-action groups share ONE
+    persistent launch; every system's result equals its own single call."""
+    groups = [c for c in CASES if c.net.kind == W.NET_MASS_ACTION and c.net.linear is None]
+    groups += [CTA[0], CTA[2], CASES[1]]
+    got = lib.integrate_batch(groups, "sie", solver, "device")
+    n0 = lib.launch_count()
+    lib.integrate_batch(groups, "sie", solver, "device")
+    assert lib.launch_count() - n0 == 2  # one mixed-size launch + one lane launch
+    for (yg, sg, ng), wl in zip(got, groups):
+        y = wl.y0.copy()
+        _, st, n = lib.integrate(wl.net, y, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", solver,
+                                 "device")
+        assert np.array_equal(yg, y), wl.label
+        assert np.array_equal(ng, n) and np.array_equal(sg, st)

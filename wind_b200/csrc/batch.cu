@@ -1,12 +1,17 @@
 // batch.cu -- several network shapes integrated together.
+//
+// Mass-action groups of every size go to ONE persistent launch (k_mixed:
+// largest N first, each group's systems pulled from its own device work
+// queue).  Groups of the builtin networks (thread-per-system kernels) run on
+// forked streams beside it.  The caller's stream waits for all of them.
 #include <vector>
 
 #include "api_internal.h"
 
 namespace wind {
 
-// Each group runs its kernel family on its own forked stream so the groups
-// overlap on the device; the caller's stream waits for all of them.
+wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, cudaStream_t stream);
+
 wind_status launch_batch(const wind_options& o, const wind_group* groups, int ngroups,
                          cudaStream_t stream) {
     for (int g = 0; g < ngroups; g++) {
@@ -26,17 +31,9 @@ wind_status launch_batch(const wind_options& o, const wind_group* groups, int ng
     if (cudaMallocAsync((void**)&counters, (size_t)ngroups * CNT_SLOTS * 8, stream) != cudaSuccess)
         return WIND_ERR_NOMEM;
     cudaMemsetAsync(counters, 0, (size_t)ngroups * CNT_SLOTS * 8, stream);
-    cudaEvent_t fork;
-    cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
-    cudaEventRecord(fork, stream);
-    std::vector<cudaStream_t> ss(ngroups, nullptr);
-    std::vector<cudaEvent_t> done(ngroups, nullptr);
-    wind_status st = WIND_OK;
-    for (int g = 0; g < ngroups && st == WIND_OK; g++) {
+    std::vector<KParams> mass, builtin;
+    for (int g = 0; g < ngroups; g++) {
         const wind_group& G = groups[g];
-        cudaStreamCreateWithFlags(&ss[g], cudaStreamNonBlocking);
-        cudaEventCreateWithFlags(&done[g], cudaEventDisableTiming);
-        cudaStreamWaitEvent(ss[g], fork, 0);
         KParams p{};
         p.kind = G.net.kind;
         p.n_eq = G.net.n_eq;
@@ -58,16 +55,33 @@ wind_status launch_batch(const wind_options& o, const wind_group* groups, int ng
         p.counters = counters + (size_t)g * CNT_SLOTS;
         p.max_attempts = o.max_attempts > 0 ? o.max_attempts : ((int64_t)1 << 40);
         p.timeout_ns = o.timeout_s > 0 ? (uint64_t)(o.timeout_s * 1e9) : 0;
-        st = launch_integrate(o, p, ss[g]);
-        cudaEventRecord(done[g], ss[g]);
-        cudaStreamWaitEvent(stream, done[g], 0);
+        if (p.nsys == 0) continue;
+        (p.kind == WIND_NET_MASS_ACTION ? mass : builtin).push_back(p);
     }
+    wind_status st = WIND_OK;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaStream_t> ss(builtin.size(), nullptr);
+    std::vector<cudaEvent_t> done(builtin.size(), nullptr);
+    if (!builtin.empty()) {
+        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        cudaEventRecord(fork, stream);
+    }
+    for (size_t g = 0; g < builtin.size() && st == WIND_OK; g++) {
+        cudaStreamCreateWithFlags(&ss[g], cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&done[g], cudaEventDisableTiming);
+        cudaStreamWaitEvent(ss[g], fork, 0);
+        st = launch_integrate(o, builtin[g], ss[g]);
+        cudaEventRecord(done[g], ss[g]);
+    }
+    if (st == WIND_OK) st = launch_mixed(o, mass, stream);
+    for (size_t g = 0; g < builtin.size(); g++)
+        if (done[g]) cudaStreamWaitEvent(stream, done[g], 0);
     cudaFreeAsync(counters, stream);
-    for (int g = 0; g < ngroups; g++) {
+    for (size_t g = 0; g < builtin.size(); g++) {
         if (ss[g]) cudaStreamDestroy(ss[g]);
         if (done[g]) cudaEventDestroy(done[g]);
     }
-    cudaEventDestroy(fork);
+    if (fork) cudaEventDestroy(fork);
     return st;
 }
 

@@ -364,9 +364,11 @@ __device__ void cta_substep(const CtaCtx& c, double h, void* mat, int ldA, doubl
     __syncthreads();
 }
 
+// The persistent CTA loop over one group's systems (blockDim.x must be
+// CTA_THREADS).  `gscratch` holds one matrix slot per block when the layout
+// does not keep the matrix in shared memory (and always for GJE_F64).
 template <int METHOD, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(CTA_THREADS) k_cta(const KParams p, double* gscratch, int smem_cap) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_raw, double* gscratch, int smem_cap) {
     constexpr int CAP = Cap<METHOD, CTRL>::value;
     const int N = p.n_eq, R = p.n_react, tid = threadIdx.x;
     const bool lin = p.linear != nullptr;
@@ -514,6 +516,12 @@ __global__ void __launch_bounds__(CTA_THREADS) k_cta(const KParams p, double* gs
         }
         __syncthreads();
     }
+}
+
+template <int METHOD, int CTRL, int SOLVER>
+__global__ void __launch_bounds__(CTA_THREADS) k_cta(const KParams p, double* gscratch, int smem_cap) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, smem_cap);
 }
 
 }  // namespace wind

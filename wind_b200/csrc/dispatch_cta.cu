@@ -12,11 +12,13 @@ using CtaFn = void (*)(KParams, double*, int);
 
 template <int METHOD, int CTRL>
 static CtaFn cta_by_solver(int solver) {
-    if (METHOD == WIND_METHOD_RK2) return k_cta<METHOD, CTRL, WIND_SOLVER_LU_F64>;
-    switch (solver) {
-    case WIND_SOLVER_GJE_F64: return k_cta<METHOD, CTRL, WIND_SOLVER_GJE_F64>;
-    case WIND_SOLVER_LU_F64: return k_cta<METHOD, CTRL, WIND_SOLVER_LU_F64>;
-    default: return k_cta<METHOD, CTRL, WIND_SOLVER_MIXED>;
+    if constexpr (METHOD == WIND_METHOD_RK2) return k_cta<METHOD, CTRL, WIND_SOLVER_LU_F64>;
+    else {
+        switch (solver) {
+        case WIND_SOLVER_GJE_F64: return k_cta<METHOD, CTRL, WIND_SOLVER_GJE_F64>;
+        case WIND_SOLVER_LU_F64: return k_cta<METHOD, CTRL, WIND_SOLVER_LU_F64>;
+        default: return k_cta<METHOD, CTRL, WIND_SOLVER_MIXED>;
+        }
     }
 }
 

@@ -12,11 +12,13 @@ using LaneFn = void (*)(KParams, int);
 
 template <class Net, int METHOD, int CTRL>
 static LaneFn lane_by_solver(int solver) {
-    if (METHOD == WIND_METHOD_RK2) return k_lane<Net, METHOD, CTRL, 0>;
-    switch (solver) {
-    case WIND_SOLVER_GJE_F64: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_GJE_F64>;
-    case WIND_SOLVER_LU_F64: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_LU_F64>;
-    default: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_MIXED>;
+    if constexpr (METHOD == WIND_METHOD_RK2) return k_lane<Net, METHOD, CTRL, 0>;
+    else {
+        switch (solver) {
+        case WIND_SOLVER_GJE_F64: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_GJE_F64>;
+        case WIND_SOLVER_LU_F64: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_LU_F64>;
+        default: return k_lane<Net, METHOD, CTRL, WIND_SOLVER_MIXED>;
+        }
     }
 }
 template <class Net>

@@ -9,11 +9,13 @@ using TeamFn = void (*)(KParams);
 
 template <int NMAX, int METHOD, int CTRL>
 static TeamFn team_by_solver(int solver) {
-    if (METHOD == WIND_METHOD_RK2) return k_team<NMAX, METHOD, CTRL, 0>;
-    switch (solver) {
-    case WIND_SOLVER_GJE_F64: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_GJE_F64>;
-    case WIND_SOLVER_LU_F64: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_LU_F64>;
-    default: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_MIXED>;
+    if constexpr (METHOD == WIND_METHOD_RK2) return k_team<NMAX, METHOD, CTRL, 0>;
+    else {
+        switch (solver) {
+        case WIND_SOLVER_GJE_F64: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_GJE_F64>;
+        case WIND_SOLVER_LU_F64: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_LU_F64>;
+        default: return k_team<NMAX, METHOD, CTRL, WIND_SOLVER_MIXED>;
+        }
     }
 }
 

@@ -337,9 +337,11 @@ __device__ __forceinline__ void team_take_step(const TeamCtx<NMAX>& c, double t0
     }
 }
 
+// The persistent team loop over one group's systems: every team of NMAX
+// lanes of the block takes tickets from the group's queue until it is empty.
+// `smem_raw` holds blockDim.x / NMAX team slices.
 template <int NMAX, int METHOD, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(TEAM_THREADS) k_team(const KParams p) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void team_run(const KParams& p, unsigned char* smem_raw) {
     constexpr int CAP = Cap<METHOD, CTRL>::value;
     const bool lin = p.linear != nullptr;
     const TeamLayout lay(NMAX, p.n_react, lin);
@@ -446,6 +448,12 @@ __global__ void __launch_bounds__(TEAM_THREADS) k_team(const KParams p) {
         }
         team_sync(c.mask);
     }
+}
+
+template <int NMAX, int METHOD, int CTRL, int SOLVER>
+__global__ void __launch_bounds__(TEAM_THREADS) k_team(const KParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    team_run<NMAX, METHOD, CTRL, SOLVER>(p, smem_raw);
 }
 
 }  // namespace wind
