@@ -197,6 +197,9 @@ int wind_integrate_output_steps(const wind_options* opt, const wind_network* net
 /* ---- version / diagnostics -------------------------------------------- */
 const char* wind_version(void);
 const char* wind_status_string(int status);
+/* The CUDA error behind the calling thread's last WIND_ERR_CUDA, as
+ * "<where>: <cudaError name>" ("" if none). */
+const char* wind_last_error(void);
 /* Kernel launches issued by this library since load (all entry points). */
 int64_t wind_launch_count(void);
 

@@ -136,4 +136,5 @@ def declare_api(lib: C.CDLL) -> C.CDLL:
     lib.wind_status_string.argtypes = [C.c_int]
     lib.wind_status_string.restype = C.c_char_p
     lib.wind_launch_count.restype = C.c_int64
+    lib.wind_last_error.restype = C.c_char_p
     return lib

@@ -23,6 +23,13 @@ namespace wind {
 
 std::atomic<int64_t> g_launches{0};
 
+static thread_local char t_last_error[160] = "";
+
+void record_cuda_error(cudaError_t e, const char* where) {
+    std::snprintf(t_last_error, sizeof(t_last_error), "%s: %s", where, cudaGetErrorName(e));
+}
+const char* last_error_text() { return t_last_error; }
+
 static int builtin_n(int kind) {
     switch (kind) {
     case WIND_NET_NR_TEST: return NetNR::N;
@@ -116,12 +123,15 @@ const char* wind_status_string(int s) {
 
 int64_t wind_launch_count(void) { return g_launches.load(); }
 
+const char* wind_last_error(void) { return wind::last_error_text(); }
+
 int wind_integrate(const wind_options* opt_in, const wind_network* net, double tnow,
                    double tend, int32_t n_integration_steps, double* y, int64_t nsys,
                    double atol, double rtol, int32_t* sys_status, int64_t* sys_nsteps,
                    int64_t* total_nsteps, int32_t memory, void* stream_v) {
     wind_options o;
     if (opt_in) o = *opt_in; else wind_default_options(&o);
+    (void)cudaGetLastError();  // an earlier, unrelated error is not this call's
     if (o.method != WIND_METHOD_SIE && o.method != WIND_METHOD_RK2) return WIND_ERR_ARGUMENT;
     if (o.controller != WIND_CTRL_DEVICE && o.controller != WIND_CTRL_GOLD) return WIND_ERR_ARGUMENT;
     if (o.solver < WIND_SOLVER_GJE_F64 || o.solver > WIND_SOLVER_MIXED) return WIND_ERR_ARGUMENT;
@@ -156,6 +166,7 @@ int wind_integrate_output_steps(const wind_options* opt_in, const wind_network* 
     wind_options o;
     if (opt_in) o = *opt_in; else wind_default_options(&o);
     if (n_output_steps < 1 || n_integration_steps < 1 || nsys < 0) return WIND_ERR_ARGUMENT;
+    (void)cudaGetLastError();
     if (memory != WIND_MEM_HOST && memory != WIND_MEM_DEVICE) return WIND_ERR_ARGUMENT;
     wind_status st = check_network(net, nsys);
     if (st != WIND_OK) return st;
@@ -258,5 +269,6 @@ extern "C" int wind_integrate_batch(const wind_options* opt_in, const wind_group
     wind_options o;
     if (opt_in) o = *opt_in; else wind_default_options(&o);
     if (ngroups < 0 || (ngroups > 0 && !groups)) return WIND_ERR_ARGUMENT;
+    (void)cudaGetLastError();
     return wind::launch_batch(o, groups, ngroups, (cudaStream_t)stream_v);
 }

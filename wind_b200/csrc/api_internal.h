@@ -28,6 +28,18 @@ extern std::atomic<int64_t> g_launches;
 constexpr int WIND_MAX_EQ = 256;
 constexpr int WIND_TEAM_MAX_EQ = 32;
 
+// The name of the last CUDA error this thread mapped to WIND_ERR_CUDA, with
+// the place it was seen (read back through wind_last_error()).
+void record_cuda_error(cudaError_t e, const char* where);
+const char* last_error_text();
+inline wind_status cuda_status(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return WIND_OK;
+    record_cuda_error(e, where);
+    return WIND_ERR_CUDA;
+}
+// Status of the launch just issued.
+inline wind_status launch_status(const char* where) { return cuda_status(cudaGetLastError(), where); }
+
 // True for null or for memory a kernel may dereference (device or managed).
 inline bool device_ptr(const void* ptr) {
     if (!ptr) return true;
@@ -95,7 +107,7 @@ struct IntegrateCall {
         p.counters = static_cast<unsigned long long*>(alloc(CNT_SLOTS * sizeof(unsigned long long)));
         if (failed) return WIND_ERR_NOMEM;
         if (cudaMemsetAsync(p.counters, 0, CNT_SLOTS * sizeof(unsigned long long), stream) != cudaSuccess)
-            return WIND_ERR_CUDA;
+            return launch_status("counters memset");
         if (mem == WIND_MEM_DEVICE) {
             // every array must be device (or managed) memory of a device:
             // a host pointer handed to a kernel would fault
@@ -129,7 +141,7 @@ struct IntegrateCall {
         p.y = static_cast<double*>(alloc(ybytes));
         if (failed) return WIND_ERR_NOMEM;
         if (cudaMemcpyAsync(p.y, y, ybytes, cudaMemcpyHostToDevice, stream) != cudaSuccess)
-            return WIND_ERR_CUDA;
+            return launch_status("state upload");
         if (sys_status) p.sys_status = static_cast<int32_t*>(alloc(nsys * sizeof(int32_t)));
         if (sys_nsteps) p.sys_nsteps = static_cast<int64_t*>(alloc(nsys * sizeof(int64_t)));
         if (failed) return WIND_ERR_NOMEM;
@@ -140,7 +152,7 @@ struct IntegrateCall {
         unsigned long long cnt[CNT_SLOTS] = {};
         if (memory == WIND_MEM_HOST) {
             if (cudaMemcpyAsync(h_y, params.y, ybytes, cudaMemcpyDeviceToHost, stream) != cudaSuccess)
-                return WIND_ERR_CUDA;
+                return launch_status("state download");
             if (h_status &&
                 cudaMemcpyAsync(h_status, params.sys_status, params.nsys * sizeof(int32_t),
                                 cudaMemcpyDeviceToHost, stream) != cudaSuccess)
@@ -153,10 +165,11 @@ struct IntegrateCall {
         if (memory == WIND_MEM_HOST || total) {
             if (cudaMemcpyAsync(cnt, params.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
                 return WIND_ERR_CUDA;
-            if (cudaStreamSynchronize(stream) != cudaSuccess) return WIND_ERR_CUDA;
+            const cudaError_t se = cudaStreamSynchronize(stream);
+            if (se != cudaSuccess) return cuda_status(se, "stream synchronize");
             if (total) *total = (int64_t)cnt[CNT_STEPS];
         }
-        return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
+        return launch_status("finish");
     }
 
     void release() {

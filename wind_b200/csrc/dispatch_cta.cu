@@ -83,7 +83,7 @@ wind_status launch_cta(const wind_options& o, const KParams& p, cudaStream_t str
     if (need > scratch_bytes) return WIND_ERR_NOMEM;
     fn<<<grid, CTA_THREADS, lay.bytes, stream>>>(p, need ? scratch : nullptr, cap);
     g_launches++;
-    return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
+    return launch_status("k_cta launch");
 }
 
 }  // namespace wind

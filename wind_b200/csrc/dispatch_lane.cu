@@ -78,7 +78,7 @@ wind_status launch_lane(const wind_options& o, const KParams& p, cudaStream_t st
     const int grid = (int)(need < resident ? need : resident);
     fn<<<grid, LANE_THREADS, 0, stream>>>(p, opw);
     g_launches++;
-    return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
+    return launch_status("k_lane launch");
 }
 
 }  // namespace wind

@@ -57,7 +57,8 @@ wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, 
     }
     if (smem > (size_t)cap) return WIND_ERR_UNSUPPORTED;
     MixedFn fn = mixed_fn(o.method, o.controller, o.solver);
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return launch_status("k_mixed shared-memory attribute");
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, MIXED_THREADS, smem) != cudaSuccess || nb < 1)
         return WIND_ERR_UNSUPPORTED;
@@ -83,14 +84,14 @@ wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, 
     std::memcpy(blob.data(), ps.data(), pbytes);
     std::memcpy(blob.data() + pbytes, order.data(), obytes);
     wind_status st = WIND_OK;
-    if (cudaMemcpyAsync(dparams, blob.data(), blob.size(), cudaMemcpyHostToDevice, stream) != cudaSuccess)
-        st = WIND_ERR_CUDA;
+    st = cuda_status(cudaMemcpyAsync(dparams, blob.data(), blob.size(), cudaMemcpyHostToDevice, stream),
+                     "group table upload");
     if (st == WIND_OK) {
         fn<<<grid, MIXED_THREADS, smem, stream>>>(reinterpret_cast<const KParams*>(dparams),
                                                   reinterpret_cast<const int*>(dparams + pbytes),
                                                   (int)ps.size(), gscratch, cap);
         g_launches++;
-        if (cudaGetLastError() != cudaSuccess) st = WIND_ERR_CUDA;
+        st = launch_status("k_mixed launch");
     }
     cudaFreeAsync(dparams, stream);
     if (gscratch) cudaFreeAsync(gscratch, stream);

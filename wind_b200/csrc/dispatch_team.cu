@@ -49,7 +49,7 @@ wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t st
     const int grid = (int)(need < cap ? need : cap);
     fn<<<grid, TEAM_THREADS, smem, stream>>>(p);
     g_launches++;
-    return cudaGetLastError() == cudaSuccess ? WIND_OK : WIND_ERR_CUDA;
+    return launch_status("k_team launch");
 }
 
 }  // namespace wind

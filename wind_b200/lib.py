@@ -71,7 +71,10 @@ def _is_torch(a) -> bool:
 
 def _check(code: int, what: str):
     if code != _capi.WIND_OK:
-        raise WindError(code, what)
+        detail = ""
+        if code == _capi.WIND_ERR_CUDA:
+            detail = " (" + load().wind_last_error().decode() + ")"
+        raise WindError(code, what + detail)
 
 
 def integrate(net: Network, y, tnow: float, tend: float, atol: float, rtol: float,
