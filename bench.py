@@ -221,6 +221,33 @@ def run_reference_arm(args, wl, desc):
 
 
 # ---------------------------------------------------------------------------
+def run_serve(args):
+    """Serving: seeded Poisson request streams at several rates; one JSON line
+    with p50/p99 latency and systems/s per rate."""
+    import torch
+    from wind_b200 import serve
+    torch.cuda.set_device(0)
+    rates = [float(r) for r in args.rates.split(",")]
+    out = []
+    for i, rate in enumerate(rates):
+        reqs = serve.request_stream(args.requests, seed=4 + i, max_cells=args.max_cells,
+                                    dt_range=(args.dt_lo, args.dt_hi), atol=1e-6, rtol=1e-4)
+        with serve.Server(solver=args.solver if args.solver != "auto" else "lu_f64",
+                          max_inflight=4) as srv:
+            serve.poisson_load(srv, reqs[:8], rate)  # warm-up
+            summary, _ = serve.poisson_load(srv, reqs, rate)
+            summary["launches"] = srv.stats()["launches"]
+        out.append(summary)
+    line = {"metric": METRIC, "workload": "serve", "unit": "ms",
+            "config": {"workload": (f"Poisson arrivals, {args.requests} requests per rate, cells "
+                                    f"log-U[1,{args.max_cells}], N from {{5,16,32,64,157}} at "
+                                    f"40/25/20/10/5 %, 10N reactions, dt log-U[{args.dt_lo},{args.dt_hi}], "
+                                    "atol 1e-6 rtol 1e-4, seed 4+i"),
+                       "max_inflight": 4},
+            "rates": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -235,9 +262,16 @@ def main():
     ap.add_argument("--spec-width", type=int, default=0)
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rates", default="10,30,100,300,1000,2000", help="serving request rates (Hz)")
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--max-cells", type=int, default=2000)
+    ap.add_argument("--dt-lo", type=float, default=1e-4)
+    ap.add_argument("--dt-hi", type=float, default=1e-3)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
+    if args.workload == "serve":
+        return run_serve(args)
     wl, desc = make_workload(args.workload, args.systems)
     if args.impl == "reference":
         return run_reference_arm(args, wl, desc)

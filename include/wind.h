@@ -194,6 +194,48 @@ int wind_integrate_output_steps(const wind_options* opt, const wind_network* net
                                 double* out_over_time, int64_t* steps_per_output,
                                 int32_t memory, void* stream);
 
+/* ---- serving: request loop with continuous batching --------------------- */
+/* No counterpart in the reference (its only caller integrates one batch per
+ * blocking call, python/ode_systems/ode_base.py:338-378).  A server owns a
+ * worker thread on the current device.  Requests (a set of cells of one
+ * network, an interval, tolerances; host arrays copied at submit) are
+ * admitted in arrival order while the device footprint of admitted requests
+ * stays under hbm_budget_bytes; whenever one of max_inflight launch slots is
+ * free, every admitted request not yet running -- of any network size -- is
+ * merged into one batch launch (wind_integrate_batch), so requests arriving
+ * while others run start at once and overlap with them on the device. */
+typedef struct wind_server wind_server;
+#define WIND_SERVER_MAX_GROUPS 1024  /* requests merged into one launch at most */
+typedef struct wind_server_config {
+    int32_t method, solver, controller;
+    int32_t max_inflight;        /* launch slots in flight (1..64)             */
+    int64_t hbm_budget_bytes;    /* device footprint cap of admitted requests  */
+    int64_t max_waiting;         /* waiting requests before submit says BUSY   */
+    int32_t poll_us;             /* worker idle wait                           */
+    int32_t pad_;
+} wind_server_config;
+typedef struct wind_request {
+    wind_network net;            /* host arrays                                */
+    const double* y0;            /* host [nsys*N]                              */
+    int64_t nsys;
+    double tnow, tend, atol, rtol;
+    int32_t n_integration_steps, pad_;
+} wind_request;
+void wind_server_default_config(wind_server_config* cfg);
+int wind_server_create(const wind_server_config* cfg, wind_server** out);
+/* Copies the request; WIND_ERR_BUSY when max_waiting requests wait. */
+int wind_server_submit(wind_server* srv, const wind_request* req, int64_t* id_out);
+/* Waits up to timeout_s for request `id`; on completion copies the final
+ * state, per-system status and substep counts (any may be NULL), the
+ * submit-to-completion latency, forgets the request and returns its status;
+ * WIND_ERR_TIMEOUT if it is not done yet (poll again). */
+int wind_server_poll(wind_server* srv, int64_t id, double timeout_s, double* y_out,
+                     int32_t* status_out, int64_t* nsteps_out, double* latency_s);
+/* waiting, admitted, running, completed, launches, resident bytes */
+int wind_server_stats(wind_server* srv, int64_t* out6);
+/* Finishes all submitted work, then frees the server. */
+int wind_server_destroy(wind_server* srv);
+
 /* ---- version / diagnostics -------------------------------------------- */
 const char* wind_version(void);
 const char* wind_status_string(int status);
