@@ -81,6 +81,10 @@ wind_status launch_cta(const wind_options& o, const KParams& p, cudaStream_t str
     int grid = 0;
     const size_t need = cta_scratch_bytes(o, p, &grid);
     if (need > scratch_bytes) return WIND_ERR_NOMEM;
+    // set for this launch every time (the occupancy cache may come from a
+    // launch of the same kernel with another size)
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.bytes) != cudaSuccess)
+        return launch_status("k_cta shared-memory attribute");
     fn<<<grid, CTA_THREADS, lay.bytes, stream>>>(p, need ? scratch : nullptr, cap);
     g_launches++;
     return launch_status("k_cta launch");

@@ -47,6 +47,10 @@ wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t st
     const int64_t need = (p.nsys + teams - 1) / teams;
     const int64_t cap = (int64_t)nb * device_sm_count();
     const int grid = (int)(need < cap ? need : cap);
+    // the attribute is per function, and the cached occupancy above may come
+    // from a launch with another size: set it for this launch every time
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return launch_status("k_team shared-memory attribute");
     fn<<<grid, TEAM_THREADS, smem, stream>>>(p);
     g_launches++;
     return launch_status("k_team launch");
