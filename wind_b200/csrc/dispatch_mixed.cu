@@ -52,7 +52,7 @@ wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, 
                 gslot = std::max(gslot, CtaLayout::gscratch_doubles(p.n_eq, solver));
         } else {
             const int nm = nmax_of(p.n_eq);
-            smem = std::max(smem, (size_t)(MIXED_THREADS / nm) * TeamLayout(nm, p.n_react, p.linear != nullptr).bytes);
+            smem = std::max(smem, (size_t)(MIXED_THREADS / nm) * TeamLayout(nm, p.n_react, p.linear != nullptr, solver).bytes);
         }
     }
     if (smem > (size_t)cap) return WIND_ERR_UNSUPPORTED;

@@ -15,9 +15,11 @@ TeamFn team_fn_32(int method, int ctrl, int solver);
 
 int team_nmax(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : 32); }
 
-size_t team_smem_bytes(int n, int R, bool lin) {
+// The RK2 instantiations are compiled with the GJE_F64 layout (no matrix).
+size_t team_smem_bytes(int n, int R, bool lin, int method, int solver) {
     const int nmax = team_nmax(n);
-    return (size_t)(TEAM_THREADS / nmax) * TeamLayout(nmax, R, lin).bytes;
+    const int eff = (method == WIND_METHOD_RK2) ? WIND_SOLVER_GJE_F64 : solver;
+    return (size_t)(TEAM_THREADS / nmax) * TeamLayout(nmax, R, lin, eff).bytes;
 }
 
 static int team_blocks_per_sm(TeamFn fn, size_t smem) {
@@ -39,7 +41,7 @@ wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t st
     TeamFn fn = nmax == 8 ? team_fn_8(o.method, o.controller, o.solver)
               : nmax == 16 ? team_fn_16(o.method, o.controller, o.solver)
                            : team_fn_32(o.method, o.controller, o.solver);
-    const size_t smem = team_smem_bytes(p.n_eq, p.n_react, p.linear != nullptr);
+    const size_t smem = team_smem_bytes(p.n_eq, p.n_react, p.linear != nullptr, o.method, o.solver);
     if (smem > 227 * 1024) return WIND_ERR_UNSUPPORTED;
     const int nb = team_blocks_per_sm(fn, smem);
     if (nb < 1) return WIND_ERR_UNSUPPORTED;

@@ -29,17 +29,28 @@ constexpr int TEAM_THREADS = 128;
 constexpr int TEAM_MAXN = 32;
 
 struct TeamLayout {
-    // byte offsets inside one team's shared slice
-    int js, bc, vec, lt, rates, species, bytes;
+    // byte offsets inside one team's shared slice.  GJE_F64 keeps the FP64
+    // Jacobian Js (reference orientation) and the broadcast rows; LU_F64 and
+    // MIXED keep the matrix A = I - hJ row-major with the right-hand side as
+    // column N (leading dimension NMAX+1: odd, so the lanes' rows fall in
+    // distinct banks), the per-species reaction incidence lists and the pivot
+    // order.
+    int js, bc, vec, lt, rates, species, mat, inc_off, inc, piv, bytes;
     __host__ __device__ static int align16(int x) { return (x + 15) & ~15; }
-    __host__ __device__ TeamLayout(int nmax, int R, bool lin) {
+    __host__ __device__ TeamLayout(int nmax, int R, bool lin, int solver = WIND_SOLVER_GJE_F64) {
+        const bool gje = (solver == WIND_SOLVER_GJE_F64);
+        const int esz = (solver == WIND_SOLVER_MIXED) ? 4 : 8;
         int off = 0;
-        js = off; off = align16(off + nmax * nmax * 8);
-        bc = off; off = align16(off + 2 * (2 * nmax + 4) * 8);
-        vec = off; off = align16(off + 8 * nmax * 8);
+        js = off; off = align16(off + (gje ? nmax * nmax * 8 : 0));
+        bc = off; off = align16(off + (gje ? 2 * (2 * nmax + 4) * 8 : 0));
+        vec = off; off = align16(off + 10 * nmax * 8);
         lt = off; off = align16(off + (lin ? nmax * nmax * 4 : 0));
         rates = off; off = align16(off + R * 8);
         species = off; off = align16(off + R * 4 * 2);
+        mat = off; off = align16(off + (gje ? 0 : nmax * (nmax + 1) * esz));
+        inc_off = off; off = align16(off + (gje ? 0 : (nmax + 1) * 4));
+        inc = off; off = align16(off + (gje ? 0 : 4 * R * 2));
+        piv = off; off = align16(off + (gje ? 0 : nmax * 4));
         bytes = off;
     }
 };
@@ -64,6 +75,11 @@ struct TeamCtx {
     float* LT;      // [NMAX*NMAX] LT[i*NMAX+j] = L[j][i], or null
     double* rates;  // [R]
     const uint16_t* sp;  // [R*4]
+    void* A;        // [NMAX*(NMAX+1)] LU/MIXED matrix (double or float)
+    int* inc_off;   // [NMAX+1] CSR offsets
+    uint16_t* inc;  // CSR reaction ids
+    int* piv;       // [NMAX] lane chosen at pivot step i
+    double* r;      // [NMAX] refinement residual
 };
 
 // f_l and column l of Jt for the current v (mass action + optional L).
@@ -286,6 +302,138 @@ struct TeamLU {
     }
 };
 
+// f_l and, with JAC, row l of A = I - hJ (standard orientation, J[l][c] =
+// d f_l / d y_c) with f_l as column N, from the CSR incidence list of species
+// l: the per-element update sequence is the sequential one of the
+// mass-action contract (reactions ascending).
+template <int NMAX, typename T, bool JAC>
+__device__ __forceinline__ void team_rhs_row(const TeamCtx<NMAX>& c, double h) {
+    constexpr int ld = NMAX + 1;
+    const int l = c.l, N = c.N;
+    if (l < N) {
+        T* row = static_cast<T*>(c.A) + l * ld;
+        xd acc = 0.0;
+        if (c.LT)
+            for (int k = 0; k < N; k++) acc += xd((double)c.LT[k * NMAX + l]) * xd(c.v[k]);
+        if (JAC)
+            for (int cc = 0; cc < N; cc++) row[cc] = c.LT ? (T)c.LT[cc * NMAX + l] : (T)0;
+        const int e1 = c.inc_off[l + 1];
+        for (int e = c.inc_off[l]; e < e1; e++) {
+            const int rr = c.inc[e];
+            const uint2 q = *reinterpret_cast<const uint2*>(c.sp + 4 * rr);
+            const int a = q.x & 0xffff, b = q.x >> 16, cc = q.y & 0xffff, d = q.y >> 16;
+            const xd k = c.rates[rr];
+            const xd ya = c.v[a], yb = c.v[b];
+            const xd w = k * ya * yb;
+            if (a == l) acc -= w;
+            if (b == l) acc -= w;
+            if (cc == l) acc += w;
+            if (d == l) acc += w;
+            if (JAC) {
+                const xd da = k * yb, db = k * ya;
+                if (a == l) row[a] = (T)(xd((double)row[a]) - da);
+                if (b == l) row[a] = (T)(xd((double)row[a]) - da);
+                if (cc == l) row[a] = (T)(xd((double)row[a]) + da);
+                if (d == l) row[a] = (T)(xd((double)row[a]) + da);
+                if (a == l) row[b] = (T)(xd((double)row[b]) - db);
+                if (b == l) row[b] = (T)(xd((double)row[b]) - db);
+                if (cc == l) row[b] = (T)(xd((double)row[b]) + db);
+                if (d == l) row[b] = (T)(xd((double)row[b]) + db);
+            }
+        }
+        c.f[l] = acc.v;
+        if (JAC) {
+            for (int cc = 0; cc < N; cc++) row[cc] = (T)((cc == l ? 1.0 : 0.0) - h * (double)row[cc]);
+            row[N] = (T)acc.v;
+        }
+    }
+    team_sync(c.mask);
+}
+
+// (J x)_l in FP64 from the reactions and L (refinement residual).
+template <int NMAX>
+__device__ __forceinline__ double team_jx(const TeamCtx<NMAX>& c, const double* xv) {
+    const int l = c.l, N = c.N;
+    double acc = 0.0;
+    if (c.LT)
+        for (int k = 0; k < N; k++) acc = fma((double)c.LT[k * NMAX + l], xv[k], acc);
+    const int e1 = c.inc_off[l + 1];
+    for (int e = c.inc_off[l]; e < e1; e++) {
+        const int rr = c.inc[e];
+        const uint2 q = *reinterpret_cast<const uint2*>(c.sp + 4 * rr);
+        const int a = q.x & 0xffff, b = q.x >> 16, cc = q.y & 0xffff, d = q.y >> 16;
+        const double dw = c.rates[rr] * (c.v[b] * xv[a] + c.v[a] * xv[b]);
+        if (a == l) acc -= dw;
+        if (b == l) acc -= dw;
+        if (cc == l) acc += dw;
+        if (d == l) acc += dw;
+    }
+    return acc;
+}
+
+// Partial-pivot LU of A (shared memory, lane l owns row l, rows never move)
+// and the solve of its right-hand side column N.  Step i: one warp reduction
+// picks the pivot lane p, every active lane reads the pivot row straight from
+// shared memory and updates its own row.  Loops stay rolled, so the code is
+// small for every N.  Returns this lane's pivot step (-1 for l >= N); x in c.x.
+template <int NMAX, typename T, bool STORE_L>
+__device__ __forceinline__ int team_lu_smem(const TeamCtx<NMAX>& c) {
+    constexpr int ld = NMAX + 1;
+    const int l = c.l, N = c.N;
+    T* A = static_cast<T*>(c.A);
+    T* my = A + l * ld;
+    int mystep = (l < N) ? NMAX : -1;
+    for (int i = 0; i < N; i++) {
+        const unsigned key = pivot_key((double)my[i], l, mystep == NMAX);
+        const int p = 31 - (int)(__reduce_max_sync(c.mask, key) & 31u);
+        const T* prow = A + p * ld;
+        if (l == p) {
+            mystep = i;
+            c.piv[i] = p;
+        } else if (mystep == NMAX) {
+            const T lk = my[i] * nr_rcp(prow[i]);
+            if (STORE_L) my[i] = lk;
+            for (int t = i + 1; t <= N; t++) my[t] = fma(-lk, prow[t], my[t]);
+        }
+        team_sync(c.mask);
+    }
+    // back substitution, column-oriented: x_i from the pivot lane of step i
+    double z = (l < N) ? (double)my[N] : 0.0, xl = 0.0;
+    for (int i = N - 1; i >= 0; i--) {
+        const int p = c.piv[i];
+        double xi = (l == p) ? z * (double)nr_rcp(my[i]) : 0.0;
+        xi = __shfl_sync(c.mask, xi, c.leader + p);
+        if (mystep >= 0 && mystep < i) z = fma(-(double)my[i], xi, z);
+        if (l == i) xl = xi;
+    }
+    if (l < N) c.x[l] = xl;
+    team_sync(c.mask);
+    return mystep;
+}
+
+// Re-solve with the stored factors (STORE_L) for right-hand side r (this
+// lane's row, original order); result in c.x.
+template <int NMAX, typename T>
+__device__ __forceinline__ void team_lu_resolve(const TeamCtx<NMAX>& c, int mystep, double r) {
+    constexpr int ld = NMAX + 1;
+    const int l = c.l, N = c.N;
+    const T* my = static_cast<const T*>(c.A) + l * ld;
+    for (int i = 0; i < N; i++) {
+        const double rp = __shfl_sync(c.mask, r, c.leader + c.piv[i]);
+        if (mystep > i) r = fma(-(double)my[i], rp, r);
+    }
+    double xl = 0.0;
+    for (int i = N - 1; i >= 0; i--) {
+        const int p = c.piv[i];
+        double xi = (l == p) ? r * (double)nr_rcp(my[i]) : 0.0;
+        xi = __shfl_sync(c.mask, xi, c.leader + p);
+        if (mystep >= 0 && mystep < i) r = fma(-(double)my[i], xi, r);
+        if (l == i) xl = xi;
+    }
+    if (l < N) c.x[l] = xl;
+    team_sync(c.mask);
+}
+
 template <int NMAX, int METHOD, int CTRL, int SOLVER>
 __device__ __forceinline__ void team_substep(const TeamCtx<NMAX>& c, double h) {
     if (METHOD == WIND_METHOD_RK2) {
@@ -294,30 +442,28 @@ __device__ __forceinline__ void team_substep(const TeamCtx<NMAX>& c, double h) {
         team_sync(c.mask);
         return;
     }
-    team_rhs_jac<NMAX, true>(c);
     if (SOLVER == WIND_SOLVER_GJE_F64) {
+        team_rhs_jac<NMAX, true>(c);
         team_gje_exact<NMAX, CTRL>(c, h);
         return;
     }
     if (SOLVER == WIND_SOLVER_LU_F64) {
-        TeamLU<NMAX, double> lu;
-        lu.factor_solve(c, h);
+        team_rhs_row<NMAX, double, true>(c, h);
+        team_lu_smem<NMAX, double, false>(c);
         if (c.l < c.N) c.v[c.l] = c.v[c.l] + h * c.x[c.l];
         team_sync(c.mask);
         return;
     }
-    TeamLU<NMAX, float> lu;
-    lu.factor_solve(c, h);
-    // residual r = f - (x - h J x) in FP64 from the shared FP64 Jacobian
-    double r = 0.0;
+    // MIXED: FP32 factors, one FP64 refinement step with r = f - (x - h J x)
+    team_rhs_row<NMAX, float, true>(c, h);
+    const int mystep = team_lu_smem<NMAX, float, true>(c);
+    double r = 0.0, x0 = 0.0;
     if (c.l < c.N) {
-        double jx = 0.0;
-        for (int i = 0; i < c.N; i++) jx = fma(c.Js[i * NMAX + c.l], c.x[i], jx);
-        r = c.f[c.l] - (c.x[c.l] - h * jx);
+        x0 = c.x[c.l];
+        r = c.f[c.l] - (x0 - h * team_jx(c, c.x));
     }
-    const double x0 = (c.l < c.N) ? c.x[c.l] : 0.0;
     team_sync(c.mask);
-    lu.resolve(c, r);
+    team_lu_resolve<NMAX, float>(c, mystep, r);
     if (c.l < c.N) c.v[c.l] = c.v[c.l] + h * (x0 + c.x[c.l]);
     team_sync(c.mask);
 }
@@ -344,7 +490,7 @@ template <int NMAX, int METHOD, int CTRL, int SOLVER>
 __device__ __forceinline__ void team_run(const KParams& p, unsigned char* smem_raw) {
     constexpr int CAP = Cap<METHOD, CTRL>::value;
     const bool lin = p.linear != nullptr;
-    const TeamLayout lay(NMAX, p.n_react, lin);
+    const TeamLayout lay(NMAX, p.n_react, lin, SOLVER);
     const int team = threadIdx.x / NMAX;
     const int lane = threadIdx.x & 31;
     TeamCtx<NMAX> c;
@@ -367,6 +513,11 @@ __device__ __forceinline__ void team_run(const KParams& p, unsigned char* smem_r
     c.rates = reinterpret_cast<double*>(base + lay.rates);
     uint16_t* sp_s = reinterpret_cast<uint16_t*>(base + lay.species);
     c.sp = sp_s;
+    c.A = base + lay.mat;
+    c.inc_off = reinterpret_cast<int*>(base + lay.inc_off);
+    c.inc = reinterpret_cast<uint16_t*>(base + lay.inc);
+    c.piv = reinterpret_cast<int*>(base + lay.piv);
+    c.r = vec + 6 * NMAX;
     const int N = c.N, R = c.R, l = c.l;
     const uint64_t t_start = p.timeout_ns ? global_ns() : 0;
 
@@ -390,6 +541,34 @@ __device__ __forceinline__ void team_run(const KParams& p, unsigned char* smem_r
             *reinterpret_cast<uint2*>(sp_s + 4 * r) = q;
         }
         bad_idx = __any_sync(c.mask, bad_idx);
+        if (SOLVER != WIND_SOLVER_GJE_F64 && !bad_idx) {
+            // per-species incidence lists (reaction ids ascending)
+            team_sync(c.mask);
+            if (l < N) {
+                int cnt = 0;
+                for (int r = 0; r < R; r++) {
+                    const uint2 q = *reinterpret_cast<const uint2*>(sp_s + 4 * r);
+                    cnt += ((q.x & 0xffff) == (unsigned)l) | ((q.x >> 16) == (unsigned)l) |
+                           ((q.y & 0xffff) == (unsigned)l) | ((q.y >> 16) == (unsigned)l);
+                }
+                c.inc_off[l + 1] = cnt;
+            }
+            team_sync(c.mask);
+            if (l == 0) {
+                c.inc_off[0] = 0;
+                for (int j = 0; j < N; j++) c.inc_off[j + 1] += c.inc_off[j];
+            }
+            team_sync(c.mask);
+            if (l < N) {
+                int o = c.inc_off[l];
+                for (int r = 0; r < R; r++) {
+                    const uint2 q = *reinterpret_cast<const uint2*>(sp_s + 4 * r);
+                    if ((q.x & 0xffff) == (unsigned)l || (q.x >> 16) == (unsigned)l ||
+                        (q.y & 0xffff) == (unsigned)l || (q.y >> 16) == (unsigned)l)
+                        c.inc[o++] = (uint16_t)r;
+                }
+            }
+        }
         if (lin && l < N) {
             const float* Lg = p.linear + s * (int64_t)N * N;
             for (int k = 0; k < N; k++) c.LT[k * NMAX + l] = Lg[l * N + k];
