@@ -43,7 +43,7 @@ METRIC = "systems/s at 1e-5 rel err vs FP64 (mixed vs plain FP64 GPU); serve p50
 
 
 # ---------------------------------------------------------------------------
-def make_workload(name: str, systems: int = 0):
+def make_workload(name: str, systems: int = 0, dt: float = 0.0):
     if name == "katz96":
         n = systems or 65536
         wl = W.workload_katz96(n, atol=1e-8, rtol=1e-6)
@@ -57,8 +57,19 @@ def make_workload(name: str, systems: int = 0):
         wl = W.Workload(wl.net, wl.y0, 0.0, 0.01, wl.atol, wl.rtol, 1, 1, "nr_test")
         return wl, "NR stiff linear test, 1024 systems, one output interval t=0..0.01"
     if name == "dense":
-        wl = W.workload_dense(16384)
-        return wl, "dense N=32 + 64 reactions, 16,384 systems, dt=1, atol=1e-8 rtol=1e-6"
+        n = systems or 16384
+        wl = W.workload_dense(n)
+        t = dt or 1.0
+        wl = W.Workload(wl.net, wl.y0, 0.0, t, wl.atol, wl.rtol, 1, 1, "dense32")
+        return wl, f"dense N=32 + 64 reactions, {n:,} systems, dt={t:g}, atol=1e-8 rtol=1e-6"
+    if name.startswith("ma"):
+        # one size class of the mixed-size batch: N = int(name[2:]), 10N reactions
+        N = int(name[2:])
+        n = systems or 2048
+        t = dt or 1e-3
+        wl = W.workload_mixed(n * 20, seed=3, sizes=(N,), fractions=(1.0,), dt=t)[0].subset(slice(0, n))
+        return wl, (f"mass action N={N}, {10 * N} reactions, {n:,} systems, dt={t:g}, "
+                    "atol=1e-8 rtol=1e-6")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -257,6 +268,7 @@ def main():
     ap.add_argument("--workload", default="katz96")
     ap.add_argument("--systems", type=int, default=0, help="override the system count "
                     "(profiling runs on a small case; the headline uses the default)")
+    ap.add_argument("--dt", type=float, default=0.0, help="interval override (profiling cases)")
     ap.add_argument("--method", default="sie", choices=["sie", "rk2"])
     ap.add_argument("--solver", default="auto", choices=["auto", "gje_f64", "lu_f64", "mixed"])
     ap.add_argument("--spec-width", type=int, default=0)
@@ -272,7 +284,7 @@ def main():
 
     if args.workload == "serve":
         return run_serve(args)
-    wl, desc = make_workload(args.workload, args.systems)
+    wl, desc = make_workload(args.workload, args.systems, args.dt)
     if args.impl == "reference":
         return run_reference_arm(args, wl, desc)
 
