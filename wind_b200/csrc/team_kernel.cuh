@@ -20,6 +20,8 @@
 //           Jacobian kept in shared memory, one refinement step.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "networks.cuh"
 
@@ -47,7 +49,7 @@ struct TeamLayout {
         lt = off; off = align16(off + (lin ? nmax * nmax * 4 : 0));
         rates = off; off = align16(off + R * 8);
         species = off; off = align16(off + R * 4 * 2);
-        mat = off; off = align16(off + (gje ? 0 : nmax * (nmax + 1) * esz));
+        mat = off; off = align16(off + (gje ? 0 : nmax * (nmax + (esz == 8 ? 2 : 4)) * esz));
         inc_off = off; off = align16(off + (gje ? 0 : (nmax + 1) * 4));
         inc = off; off = align16(off + (gje ? 0 : 4 * R * 2));
         piv = off; off = align16(off + (gje ? 0 : nmax * 4));
@@ -302,13 +304,22 @@ struct TeamLU {
     }
 };
 
+// Row pitch of the shared LU matrix, in elements: a multiple of 16 bytes so
+// rows can be read as 16-byte vectors (2 doubles / 4 floats), and 16 bytes
+// more than a multiple of 128 so the 8 lanes of a quarter warp hit distinct
+// bank groups.
+template <int NMAX, typename T>
+__host__ __device__ constexpr int team_ld() {
+    return sizeof(T) == 8 ? NMAX + 2 : NMAX + 4;
+}
+
 // f_l and, with JAC, row l of A = I - hJ (standard orientation, J[l][c] =
 // d f_l / d y_c) with f_l as column N, from the CSR incidence list of species
 // l: the per-element update sequence is the sequential one of the
 // mass-action contract (reactions ascending).
 template <int NMAX, typename T, bool JAC>
 __device__ __forceinline__ void team_rhs_row(const TeamCtx<NMAX>& c, double h) {
-    constexpr int ld = NMAX + 1;
+    constexpr int ld = team_ld<NMAX, T>();
     const int l = c.l, N = c.N;
     if (l < N) {
         T* row = static_cast<T*>(c.A) + l * ld;
@@ -378,7 +389,8 @@ __device__ __forceinline__ double team_jx(const TeamCtx<NMAX>& c, const double* 
 // small for every N.  Returns this lane's pivot step (-1 for l >= N); x in c.x.
 template <int NMAX, typename T, bool STORE_L>
 __device__ __forceinline__ int team_lu_smem(const TeamCtx<NMAX>& c) {
-    constexpr int ld = NMAX + 1;
+    constexpr int ld = team_ld<NMAX, T>();
+    constexpr int V = 16 / sizeof(T);  // elements per 16-byte vector
     const int l = c.l, N = c.N;
     T* A = static_cast<T*>(c.A);
     T* my = A + l * ld;
@@ -393,7 +405,19 @@ __device__ __forceinline__ int team_lu_smem(const TeamCtx<NMAX>& c) {
         } else if (mystep == NMAX) {
             const T lk = my[i] * nr_rcp(prow[i]);
             if (STORE_L) my[i] = lk;
-            for (int t = i + 1; t <= N; t++) my[t] = fma(-lk, prow[t], my[t]);
+            // columns i+1..N in 16-byte vectors; the first vector starts at the
+            // aligned column at or below i+1 and leaves columns <= i as they are
+            using Vt = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+            for (int t0 = (i + 1) & ~(V - 1); t0 <= N; t0 += V) {
+                Vt a = *reinterpret_cast<const Vt*>(my + t0);
+                const Vt b = *reinterpret_cast<const Vt*>(prow + t0);
+                T* av = reinterpret_cast<T*>(&a);
+                const T* bv = reinterpret_cast<const T*>(&b);
+#pragma unroll
+                for (int q = 0; q < V; q++)
+                    if (t0 + q > i) av[q] = fma(-lk, bv[q], av[q]);
+                *reinterpret_cast<Vt*>(my + t0) = a;
+            }
         }
         team_sync(c.mask);
     }
@@ -415,7 +439,7 @@ __device__ __forceinline__ int team_lu_smem(const TeamCtx<NMAX>& c) {
 // lane's row, original order); result in c.x.
 template <int NMAX, typename T>
 __device__ __forceinline__ void team_lu_resolve(const TeamCtx<NMAX>& c, int mystep, double r) {
-    constexpr int ld = NMAX + 1;
+    constexpr int ld = team_ld<NMAX, T>();
     const int l = c.l, N = c.N;
     const T* my = static_cast<const T*>(c.A) + l * ld;
     for (int i = 0; i < N; i++) {
