@@ -364,11 +364,21 @@ def main():
                       "max_rel_err_vs_fp64": err}
     ok = [s for s in solvers if results[s]["max_rel_err_vs_fp64"] <= 1e-5]
     best = max(ok, key=lambda s: results[s]["systems_per_s"]) if ok else "gje_f64"
+    width = args.spec_width
+    tuning = None
+    if args.solver == "auto" and args.spec_width == 0 and net.kind != W.NET_MASS_ACTION:
+        # initial lanes per system (autotuner): widths 1..8 for the chosen solver
+        from wind_b200 import autotune
+        tbest, table = autotune.tune(wl, args.method, "device", widths=(1, 2, 4, 8),
+                                     solvers=(best,))
+        tuning = table
+        if tbest["solver"] == best:
+            width = tbest["spec_width"]
 
     # the timed run of the chosen path
     launches0 = lib.launch_count()
     with ClockSampler(local) as clk:
-        times, nsub = timed(best, args.spec_width, args.steps, args.warmup)
+        times, nsub = timed(best, width, args.steps, args.warmup)
     launches = lib.launch_count() - launches0
     launches = launches * args.steps // (args.steps + args.warmup)
     tot = sum(times)
@@ -385,7 +395,7 @@ def main():
     h_arr = {k: torch.from_numpy(np.ascontiguousarray(getattr(net, k))).pin_memory()
              for k in ("constants", "rates", "species", "linear") if getattr(net, k) is not None}
     hns = _capi.network_struct(net, h_arr)
-    o = lib.options(args.method, best, "device", args.spec_width)
+    o = lib.options(args.method, best, "device", width)
     e2e_times = []
     for i in range(args.warmup + args.steps):
         h_y.copy_(h_y0)
@@ -449,7 +459,7 @@ def main():
                        "controller": "device (cuda/common/kernel.cu semantics)",
                        "systems": net.nsys, "equations": N, "l2": "flushed (256 MB write) between steps",
                        "parallelism": f"replicas x{world}"},
-            "solvers": results,
+            "solvers": results, "spec_width": width, "tuning": tuning,
             "max_rel_err_vs_fp64": results[best]["max_rel_err_vs_fp64"],
             "e2e": {"value": world * net.nsys * args.steps / e2e_tot, "unit": "systems/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
