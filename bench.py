@@ -232,6 +232,51 @@ def run_reference_arm(args, wl, desc):
 
 
 # ---------------------------------------------------------------------------
+def run_mixed(args):
+    """The mixed-size batch (N in {5,16,32,64,157} at 40/25/20/10/5 %, 10N
+    reactions) through wind_integrate_batch -- one persistent launch for all
+    sizes -- timed with CUDA events per solver; one JSON line with systems/s
+    per solver, the MIXED/LU_F64 ratio and MIXED's error vs LU_F64."""
+    import torch
+    from wind_b200 import lib
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    nsys = args.systems or 200000
+    dt = args.dt or 1e-4
+    groups = W.workload_mixed(nsys, seed=3, dt=dt, atol=1e-8, rtol=1e-6)
+    res, ys = {}, {}
+    for solver in ("lu_f64", "mixed"):
+        times = []
+        for i in range(args.warmup + args.steps):
+            dg = [lib.DeviceGroup(wl, dev) for wl in groups]
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            stream = torch.cuda.current_stream(dev)
+            arr = (lib._capi.WindGroup * len(dg))(*[g.struct() for g in dg])
+            o = lib.options("sie", solver, "device")
+            e0.record(stream)
+            code = lib.load().wind_integrate_batch(lib.C.byref(o), arr, len(dg), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            if code != 0:
+                raise RuntimeError(f"wind_integrate_batch failed: {code}")
+            if i >= args.warmup:
+                times.append(e0.elapsed_time(e1) * 1e-3)
+        ys[solver] = np.concatenate([g.y.cpu().numpy().ravel() for g in dg])
+        res[solver] = {"systems_per_s": nsys / statistics.median(times),
+                       "ms_per_step": 1e3 * statistics.median(times)}
+    a, b = ys["mixed"], ys["lu_f64"]
+    err = float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-8)))
+    line = {"metric": METRIC, "workload": "mixed", "unit": "systems/s",
+            "value": res["mixed"]["systems_per_s"], "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": (f"{nsys:,} systems, N in {{5,16,32,64,157}} at 40/25/20/10/5 %, "
+                                    f"10N reactions, dt={dt:g}, atol 1e-8 rtol 1e-6, one persistent "
+                                    "launch (wind_integrate_batch)")},
+            "solvers": res, "mixed_over_fp64": res["mixed"]["systems_per_s"] / res["lu_f64"]["systems_per_s"],
+            "max_rel_err_mixed_vs_fp64": err}
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args):
     """Serving: seeded Poisson request streams at several rates; one JSON line
     with p50/p99 latency and systems/s per rate."""
@@ -284,6 +329,8 @@ def main():
 
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "mixed":
+        return run_mixed(args)
     wl, desc = make_workload(args.workload, args.systems, args.dt)
     if args.impl == "reference":
         return run_reference_arm(args, wl, desc)

@@ -139,6 +139,30 @@ __device__ __forceinline__ void lane_take_step(const double (&c)[Net::NC], doubl
     }
 }
 
+// One attempt: the full step into y1 and the two half steps into y2, written
+// as straight-line code so the full step and the first half step -- which
+// are independent -- can be interleaved by the scheduler; the attempt's
+// critical path is then two substeps instead of three.  Each substep is the
+// same arithmetic as lane_take_step's (take_step, sie_gold.c:38-51;
+// innerstep, kernel.cu:69-91).
+template <class Net, int METHOD, int CTRL, int SOLVER>
+__device__ __forceinline__ void lane_attempt(const double (&c)[Net::NC], double t0, double H,
+                                             xd (&y1)[Net::N], xd (&y2)[Net::N]) {
+    const double t1 = t0 + H;
+    double hf = (t1 - t0) * 1.0;
+    double hh = (t1 - t0) * 0.5;
+    if (CTRL == WIND_CTRL_DEVICE) {
+        hf = fmin(t1 - t0, hf);
+        hh = fmin(t1 - t0, hh);
+    }
+    lane_substep<Net, METHOD, CTRL, SOLVER>(c, xd(hf), y1);
+    lane_substep<Net, METHOD, CTRL, SOLVER>(c, xd(hh), y2);
+    const double tm = t0 + hh;
+    double hh2 = hh;
+    if (CTRL == WIND_CTRL_DEVICE) hh2 = fmin(t1 - tm, hh);
+    lane_substep<Net, METHOD, CTRL, SOLVER>(c, xd(hh2), y2);
+}
+
 // Lanes of the warp that point at the same owner form a team.  With a
 // systems in the warp (owners), lane i works on owner (i mod a) at
 // refinement level (i div a): lanes are spread round-robin, so team sizes
@@ -260,8 +284,7 @@ __global__ void __launch_bounds__(LANE_THREADS) k_lane(const KParams p, const in
         for (int i = 0; i < N; i++) { y1[i] = y[i]; y2[i] = y[i]; }
         bool err = true;
         if (valid) {
-            lane_take_step<Net, METHOD, CTRL, SOLVER>(c, t_j, hl, 1, y1);
-            lane_take_step<Net, METHOD, CTRL, SOLVER>(c, t_j, hl, 2, y2);
+            lane_attempt<Net, METHOD, CTRL, SOLVER>(c, t_j, hl, y1, y2);
             err = false;
 #pragma unroll
             for (int i = 0; i < N; i++) err |= elem_error<METHOD, CTRL>(y1[i], y2[i], p.atol, p.rtol);
