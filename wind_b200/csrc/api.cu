@@ -80,12 +80,14 @@ wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream
     if (p.n_eq <= WIND_TEAM_MAX_EQ) return launch_team(o, p, stream);
     // CTA kernels: global scratch for the matrices that do not fit in shared
     // memory, taken from the stream-ordered pool and returned after the launch
-    const size_t need = cta_scratch_bytes(o, p, nullptr);
-    if (need == 0) return launch_cta(o, p, stream, nullptr, 0);
-    if (!allow_alloc) return WIND_ERR_UNSUPPORTED;
+    CtaPlan pl;
+    const wind_status pst = plan_cta(o, p, allow_alloc, &pl);
+    if (pst != WIND_OK) return pst;
+    if (pl.gstride == 0) return launch_cta(pl, p, stream, nullptr);
     double* scratch = nullptr;
-    if (cudaMallocAsync((void**)&scratch, need, stream) != cudaSuccess) return WIND_ERR_NOMEM;
-    const wind_status st = launch_cta(o, p, stream, scratch, need);
+    if (cudaMallocAsync((void**)&scratch, (size_t)pl.grid * pl.gstride * sizeof(double), stream) != cudaSuccess)
+        return WIND_ERR_NOMEM;
+    const wind_status st = launch_cta(pl, p, stream, scratch);
     cudaFreeAsync(scratch, stream);
     return st;
 }

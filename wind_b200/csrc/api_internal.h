@@ -19,9 +19,15 @@ wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream
                              bool allow_alloc = true);
 wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream);
 wind_status launch_lane(const wind_options& o, const KParams& p, cudaStream_t stream);
-size_t cta_scratch_bytes(const wind_options& o, const KParams& p, int* grid_out);
-wind_status launch_cta(const wind_options& o, const KParams& p, cudaStream_t stream, double* scratch,
-                       size_t scratch_bytes);
+// A CTA-kernel launch: kernel, shared-memory budget and size, grid, and
+// the per-block global scratch (doubles; 0 = none).
+struct CtaPlan {
+    const void* fn;
+    int smem_cap, smem_bytes, grid;
+    size_t gstride;
+};
+wind_status plan_cta(const wind_options& o, const KParams& p, bool allow_global, CtaPlan* out);
+wind_status launch_cta(const CtaPlan& pl, const KParams& p, cudaStream_t stream, double* scratch);
 extern std::atomic<int64_t> g_launches;
 // Largest N any kernel family accepts (lane/team kernels up to 32, CTA
 // kernels up to 256).

@@ -2,24 +2,42 @@
 // networks with 32 < N <= 256 (the 64- and 157-species classes).
 //
 // One CTA (256 threads) integrates one system at a time and pulls the next
-// ticket from the device work queue when it finishes.  Per system it stages
-// in shared memory: the state vectors, the dense linear term (transposed,
-// FP32) if any, and per-species incidence lists of the reactions (CSR,
-// reaction ids ascending), so thread j evaluates f_j and row j of the
-// Jacobian from the ~4R/N reactions that touch species j instead of all R.
+// ticket from the device work queue when it finishes.  Thread l owns
+// equation l (N <= 256): its y, y1, y2 live in registers.  Per system the CTA
+// builds per-species incidence lists of the reactions (CSR, reaction ids
+// ascending), so thread j evaluates f_j and row j of the Jacobian from the
+// ~4R/N reactions that touch species j instead of all R.
 //
 // Solvers (selected at compile time):
 //  GJE_F64  the reference's unpivoted Gauss-Jordan inverse, reference
 //           operation order, on M and Inv in a per-CTA global scratch slot
 //           (2 N^2 doubles; L2-resident) -- bit-exact parity path;
-//  LU_F64   right-looking LU with partial pivoting on the matrix in shared
-//           memory (global scratch when N^2 doubles do not fit), rows
-//           permuted implicitly (no row moves), the right-hand side carried as
-//           column N, two CTA barriers per pivot;
-//  MIXED    the same LU with FP32 factors in shared memory, FP64 residual
-//           r = f - (x - h J x) evaluated from the reactions (no FP64
-//           matrix), two FP64 refinement steps.
+//  LU_F64   blocked right-looking LU with partial pivoting, FP64, on the
+//           matrix [A | b] in shared memory (global scratch when it does not
+//           fit), followed by blocked triangular solves;
+//  MIXED    the same LU with FP32 factors, FP64 residual r = f - (x - h J x)
+//           evaluated from the reactions (no FP64 matrix), two FP64
+//           refinement steps with the FP32 factors.  Its footprint lets two
+//           CTAs share an SM at N = 157.
+//
+// Blocked LU (panel width CTA_NB = 16).  Rows never move: logical row i is
+// physical row piv[i].  For each panel:
+//  1. panel factorisation: thread p holds the 16 panel entries of physical
+//     row p in registers.  Per column one CTA barrier: each warp's best
+//     candidate (max |a| by a __reduce_max_sync key, lowest row on ties)
+//     publishes its row's panel entries in a per-warp slot (double-
+//     buffered), every thread then picks the best slot and eliminates its
+//     own row in registers;
+//  2. the still-active rows are compacted into act[] (warp ballots);
+//  3. U12 = L11^-1 A12 for the 16 pivot rows, one thread per column;
+//  4. trailing update A22 -= L21 U12 over act[] x columns, 4x4 register
+//     tiles with 16-byte shared-memory vectors.
+// The right-hand side is column N, so the forward elimination comes with the
+// factorisation; the row stride is padded so that rows start 16 bytes apart
+// in the bank space (no conflicts when 32 rows are read at one column).
 #pragma once
+
+#include <type_traits>
 
 #include "common.cuh"
 #include "networks.cuh"
@@ -27,95 +45,229 @@
 namespace wind {
 
 constexpr int CTA_THREADS = 256;
+constexpr int CTA_WARPS = CTA_THREADS / 32;
 constexpr int CTA_MAXN = 256;
+constexpr int CTA_NB = 16;  // LU panel width
 
-// Shared-memory layout of one CTA (byte offsets), computed on the host and
-// the device alike.
+// A warp's pivot candidate for one panel column.
+template <typename T>
+struct CtaCand {
+    uint32_t key;
+    int row;
+    T rcp;                      // 1 / vals[column] (computed before the vote)
+    alignas(16) T vals[CTA_NB];
+};
+
+// Shared-memory and global-scratch layout of one CTA, computed on the host
+// and the device alike.  Shared memory holds, in order of priority, the
+// vectors, the pivot bookkeeping, the dense linear term, the matrix and the
+// incidence lists; whatever does not fit under `smem_cap` goes to the CTA's
+// global scratch slot.
 struct CtaLayout {
-    int vec, piv, inc_off, inc, lt, mat, bytes;
-    bool mat_in_smem;
+    int ld;            // matrix row stride (elements)
+    int cols;          // columns that hold data (<= ld, a multiple of 4)
+    int esz;           // matrix element size (bytes)
+    int nvec;          // FP64 vectors of length N
+    int vec, piv, act, misc, cand, lt, mat, inc_off, inc, rt, spc, bytes;
+    bool mat_in_smem, inc_in_smem, data_in_smem;
+    size_t g_mat, g_inc, g_doubles;  // global slot: offsets and size in doubles
     __host__ __device__ static int a16(int x) { return (x + 15) & ~15; }
+    // columns read or written: >= N+1, whole panels, whole 4-wide tiles
+    __host__ __device__ static int data_cols(int N) {
+        const int a = (N + 15) & ~15, b = (N + 1 + 3) & ~3;
+        return a > b ? a : b;
+    }
+    // rows 16 bytes apart modulo the 128-byte bank space
+    __host__ __device__ static int row_stride(int N, int esz) {
+        const int base = data_cols(N);
+        const int per = 128 / esz, want = 16 / esz;  // elements per bank sweep / per 16 B
+        return base + ((want - base % per) + per) % per;
+    }
     __host__ __device__ CtaLayout(int N, int R, bool lin, int solver, int smem_cap) {
+        esz = (solver == WIND_SOLVER_MIXED) ? 4 : 8;
+        ld = row_stride(N, esz);
+        cols = data_cols(N);
+        nvec = (solver == WIND_SOLVER_GJE_F64) ? 3 : (solver == WIND_SOLVER_LU_F64 ? 4 : 5);
         int off = 0;
-        vec = off; off = a16(off + 10 * N * 8);            // v f y y1 y2 x r z rinv scratch
-        piv = off; off = a16(off + (2 * N + 8) * 4);       // permutation, pivot step per row, misc
-        inc_off = off; off = a16(off + (N + 1) * 4);       // CSR offsets
-        inc = off; off = a16(off + 4 * R * 2);             // CSR reaction ids (uint16)
-        lt = off; off = a16(off + (lin ? N * N * 4 : 0));  // L^T, FP32
+        vec = off; off = a16(off + nvec * N * 8);
+        piv = off; off = a16(off + N * 4);
+        act = off; off = a16(off + N * 4);
+        misc = off; off = a16(off + 2 * CTA_WARPS * 4);
+        cand = off; off = a16(off + (solver == WIND_SOLVER_GJE_F64 ? 0 : 2 * CTA_WARPS * (16 + CTA_NB * esz)));
+        lt = off; off = a16(off + (lin ? N * N * 4 : 0));
+        const int mbytes = (solver == WIND_SOLVER_GJE_F64) ? 0 : a16(N * ld * esz);
         mat = off;
-        const int esz = (solver == WIND_SOLVER_MIXED) ? 4 : 8;
-        const int mbytes = (solver == WIND_SOLVER_GJE_F64) ? 0 : a16(N * (N + 1) * esz);
         mat_in_smem = (off + mbytes) <= smem_cap;
         if (mat_in_smem) off += mbytes;
+        const int ibytes = a16((N + 1) * 4) + a16(4 * R * 2);
+        inc_off = off;
+        inc_in_smem = (off + ibytes) <= smem_cap;
+        if (inc_in_smem) {
+            inc = off + a16((N + 1) * 4);
+            off += ibytes;
+        } else {
+            inc = 0;
+        }
+        // the system's rates and species, staged once per system
+        rt = off;
+        spc = a16(off + R * 8);
+        data_in_smem = (spc + a16(R * 8)) <= smem_cap;
+        if (data_in_smem) off = spc + a16(R * 8);
         bytes = off;
-    }
-    // doubles of global scratch per CTA
-    __host__ __device__ static size_t gscratch_doubles(int N, int solver) {
-        if (solver == WIND_SOLVER_GJE_F64) return (size_t)2 * N * N;
-        if (solver == WIND_SOLVER_LU_F64) return (size_t)N * (N + 1);
-        return (size_t)(N * (N + 1) + 1) / 2;
+        // global slot: [GJE M, Inv][matrix][incidence lists]
+        size_t g = (solver == WIND_SOLVER_GJE_F64) ? (size_t)2 * N * N : 0;
+        g_mat = g;
+        if (!mat_in_smem) g += ((size_t)N * ld * esz + 15) / 16 * 2;
+        g_inc = g;
+        if (!inc_in_smem) g += ((size_t)ibytes + 15) / 16 * 2;
+        g_doubles = g;
     }
 };
 
 struct CtaCtx {
-    int N, R, tid;
+    int N, R, tid, ld, cols;
     const double* rates;     // global [R]
     const uint16_t* sp;      // global [R*4]
     const float* LT;         // smem [N*N] or null
-    const int* inc_off;      // smem [N+1]
-    const uint16_t* inc;     // smem
-    double *v, *f, *y, *y1, *y2, *x, *r, *z, *rinv, *scr;
+    const int* inc_off;      // [N+1] (shared or global)
+    const uint16_t* inc;
+    double *v, *f, *x, *r, *rinv, *scr;
     int* piv;    // logical row -> physical row
-    int* pstep;  // physical row -> step at which it became the pivot row (N = not yet)
-    int* misc;
+    int* act;    // active rows of the trailing update
+    int* misc;   // warp counts [CTA_WARPS]
+    unsigned long long* best;  // pivot vote, three rotating slots
+    void* cand;  // CtaCand<T>[2][CTA_WARPS]
 };
 
-// f_j and, with JAC, row j of A = I - h J in standard orientation (J[j][c] =
-// Jt[c][j]) with the right-hand side f_j as column N, for j = tid, tid+256...
-// Per element the update sequence is the sequential one of the mass-action
-// contract.
-template <bool JAC, typename T>
-__device__ __forceinline__ void cta_rhs_jac(const CtaCtx& c, double h, T* A, int ldA) {
-    const int N = c.N;
-    for (int j = c.tid; j < N; j += CTA_THREADS) {
+// 4 consecutive elements through 16-byte shared/global vectors.
+__device__ __forceinline__ void ld4(const float* p, float (&a)[4]) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    a[0] = t.x; a[1] = t.y; a[2] = t.z; a[3] = t.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&a)[4]) {
+    const double2 t0 = reinterpret_cast<const double2*>(p)[0];
+    const double2 t1 = reinterpret_cast<const double2*>(p)[1];
+    a[0] = t0.x; a[1] = t0.y; a[2] = t1.x; a[3] = t1.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&a)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(a[0], a[1], a[2], a[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&a)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(a[0], a[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(a[2], a[3]);
+}
+
+template <typename T>
+__device__ __forceinline__ void ld4at(const T* p, T* a) {
+    T t[4];
+    ld4(p, t);
+    a[0] = t[0]; a[1] = t[1]; a[2] = t[2]; a[3] = t[3];
+}
+template <typename T>
+__device__ __forceinline__ void st4at(T* p, const T* a) {
+    const T t[4] = {a[0], a[1], a[2], a[3]};
+    st4(p, t);
+}
+
+// Pivot ordering key: |a| as an unsigned integer (FP64: the high word, so
+// magnitudes within 2^-20 of each other tie and the lower row wins).
+__device__ __forceinline__ uint32_t mag_key(float a) { return __float_as_uint(fabsf(a)); }
+__device__ __forceinline__ uint32_t mag_key(double a) {
+    return (uint32_t)((unsigned long long)__double_as_longlong(fabs(a)) >> 32);
+}
+
+// f_j for j = tid (FP64, the sequential per-element order of the
+// mass-action contract) into c.f.
+__device__ __forceinline__ void cta_rhs(const CtaCtx& c) {
+    const int N = c.N, j = c.tid;
+    if (j < N) {
         xd acc = 0.0;
-        T* row = JAC ? A + (size_t)j * ldA : nullptr;
-        if (c.LT) {
+        if (c.LT)
             for (int k = 0; k < N; k++) acc += xd((double)c.LT[k * N + j]) * xd(c.v[k]);
-        }
-        if (JAC) {
-            // J[j][c] = Jt[c][j]; start from L[j][c] = LT[c][j] or 0
-            for (int cc = 0; cc < N; cc++) row[cc] = c.LT ? (T)c.LT[cc * N + j] : (T)0;
-        }
         const int e0 = c.inc_off[j], e1 = c.inc_off[j + 1];
         for (int e = e0; e < e1; e++) {
             const int rr = c.inc[e];
             const uint2 q = *reinterpret_cast<const uint2*>(c.sp + 4 * rr);
             const int a = q.x & 0xffff, b = q.x >> 16, cc = q.y & 0xffff, d = q.y >> 16;
-            const xd k = __ldg(c.rates + rr);
-            const xd ya = c.v[a], yb = c.v[b];
-            const xd w = k * ya * yb;
+            const xd w = xd(c.rates[rr]) * xd(c.v[a]) * xd(c.v[b]);
             if (a == j) acc -= w;
             if (b == j) acc -= w;
             if (cc == j) acc += w;
             if (d == j) acc += w;
-            if (JAC) {
-                // element (j, a) = Jt[a][j]: updates in the sequential order
-                const xd da = k * yb, db = k * ya;
-                if (a == j) row[a] = (T)(xd((double)row[a]) - da);
-                if (b == j) row[a] = (T)(xd((double)row[a]) - da);
-                if (cc == j) row[a] = (T)(xd((double)row[a]) + da);
-                if (d == j) row[a] = (T)(xd((double)row[a]) + da);
-                if (a == j) row[b] = (T)(xd((double)row[b]) - db);
-                if (b == j) row[b] = (T)(xd((double)row[b]) - db);
-                if (cc == j) row[b] = (T)(xd((double)row[b]) + db);
-                if (d == j) row[b] = (T)(xd((double)row[b]) + db);
-            }
         }
         c.f[j] = acc.v;
-        if (JAC) {
-            for (int cc = 0; cc < N; cc++) row[cc] = (T)((cc == j ? 1.0 : 0.0) - h * (double)row[cc]);
-            row[N] = (T)acc.v;  // right-hand side as column N
+    }
+    __syncthreads();
+}
+
+// Visit the reactions that touch species j (ascending ids) with up to B
+// of them in flight: fn(k, a, b, s) with the reactants a, b and the net
+// stoichiometry s = [C == j] + [D == j] - [A == j] - [B == j] (s = 0 skipped).
+// The per-system rates and species sit in L2 when shared memory is full, so
+// the loads are issued in batches before they are used.
+template <int B = 8, typename F>
+__device__ __forceinline__ void cta_incidences(const CtaCtx& c, int j, F&& fn) {
+    const int e0 = c.inc_off[j], e1 = c.inc_off[j + 1];
+    for (int e = e0; e < e1; e += B) {
+        uint2 q[B];
+        double k[B];
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            if (e + u < e1) {
+                const int rr = c.inc[e + u];
+                q[u] = *reinterpret_cast<const uint2*>(c.sp + 4 * rr);
+                k[u] = c.rates[rr];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            if (e + u < e1) {
+                const int a = q[u].x & 0xffff, b = q[u].x >> 16, cc = q[u].y & 0xffff, d = q[u].y >> 16;
+                const int sg = (cc == j) + (d == j) - (a == j) - (b == j);
+                if (sg) fn(k[u], a, b, (double)sg);
+            }
+        }
+    }
+}
+
+// [A | b] = [I - h J | f] in standard orientation (J[j][c] = Jt[c][j]), and
+// f into c.f.  Thread j owns row j: it starts the row from L (or zero),
+// accumulates f_j and the row's Jacobian entries from its reactions, then
+// scales the row and writes f_j as column N.  (The LU and mixed solvers are
+// not bit-exact by design; the reference-order evaluation is cta_rhs /
+// cta_gje_exact.)
+template <typename T>
+__device__ void cta_build(const CtaCtx& c, double h, T* A) {
+    const int N = c.N, j = c.tid, ld = c.ld;
+    const int q4 = c.cols >> 2;  // 4-wide chunks per row that hold data
+    if (j < N) {
+        T* row = A + (size_t)j * ld;
+        double acc = 0.0;
+        if (c.LT) {
+            for (int k = 0; k < c.cols; k++) row[k] = k < N ? (T)c.LT[k * N + j] : (T)0;
+            for (int k = 0; k < N; k++) acc = fma((double)c.LT[k * N + j], c.v[k], acc);
+        } else {
+            const T z4[4] = {(T)0, (T)0, (T)0, (T)0};
+            for (int q = 0; q < q4; q++) st4(row + 4 * q, z4);
+        }
+        cta_incidences<sizeof(T) == 4 ? 2 : 8>(c, j, [&](double k, int a, int b, double sg) {
+            const double ya = c.v[a], yb = c.v[b];
+            acc = fma(sg * k * ya, yb, acc);
+            row[a] = (T)((double)row[a] + sg * k * yb);
+            row[b] = (T)((double)row[b] + sg * k * ya);
+        });
+        c.f[j] = acc;
+        if (j < 3) c.best[j] = 0ull;  // pivot-vote slots of the next LU
+        for (int q = 0; q < q4; q++) {
+            T a[4];
+            ld4(row + 4 * q, a);
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int cc = 4 * q + t;
+                if (cc < N) a[t] = (T)((cc == j ? 1.0 : 0.0) - h * (double)a[t]);
+                else if (cc == N) a[t] = (T)acc;
+            }
+            st4(row + 4 * q, a);
         }
     }
     __syncthreads();
@@ -127,113 +279,223 @@ __device__ __forceinline__ double cta_jx(const CtaCtx& c, int j, const double* x
     double acc = 0.0;
     if (c.LT)
         for (int k = 0; k < N; k++) acc = fma((double)c.LT[k * N + j], xv[k], acc);
-    const int e0 = c.inc_off[j], e1 = c.inc_off[j + 1];
-    for (int e = e0; e < e1; e++) {
-        const int rr = c.inc[e];
-        const uint2 q = *reinterpret_cast<const uint2*>(c.sp + 4 * rr);
-        const int a = q.x & 0xffff, b = q.x >> 16, cc = q.y & 0xffff, d = q.y >> 16;
-        const double k = __ldg(c.rates + rr);
-        const double dw = k * (c.v[b] * xv[a] + c.v[a] * xv[b]);
-        if (a == j) acc -= dw;
-        if (b == j) acc -= dw;
-        if (cc == j) acc += dw;
-        if (d == j) acc += dw;
-    }
+    cta_incidences<4>(c, j, [&](double k, int a, int b, double sg) {
+        acc = fma(sg * k, fma(c.v[b], xv[a], c.v[a] * xv[b]), acc);
+    });
     return acc;
 }
 
-// Right-looking LU with partial pivoting on A (N rows, N+1 columns: the last
-// is the right-hand side).  Implicit row permutation piv[] (logical row i is
-// physical row piv[i]).  On return c.x holds the solution and c.rinv[i]
-// holds 1/U_ii; with STORE_L the multipliers are kept in A's column i of the
-// rows below (for later re-solves).  The multipliers of step i-1 are scaled
-// during step i's pivot search, on the rows whose pivot step is >= i (a set
-// the concurrent swap cannot change).
-template <typename T, bool STORE_L>
-__device__ void cta_lu_solve(const CtaCtx& c, T* A, int ldA) {
-    const int N = c.N, tid = c.tid;
+// Blocked right-looking LU with partial pivoting of [A | b] in place (see
+// the file comment).  On return: c.piv[i] = physical row of logical row i,
+// c.rinv[i] = 1/U_ii, the multipliers below the pivots, U above, and
+// column N holds the forward-eliminated right-hand side.
+template <typename T>
+__device__ void cta_lu(const CtaCtx& c, T* A) {
+    const int N = c.N, tid = c.tid, ld = c.ld;
     const int warp = tid >> 5, lane = tid & 31;
-    for (int i = tid; i < N; i += CTA_THREADS) {
-        c.piv[i] = i;
-        c.pstep[i] = N;
-    }
-    __syncthreads();
-    // 2-D thread grid for the trailing update
-    const int ty = tid >> 4, tx = tid & 15;
-    for (int i = 0; i < N; i++) {
-        if (warp == 0) {
-            // pivot search over logical rows i..N-1 of column i
-            double best = -1.0;
-            int bk = N;
-            for (int k = i + lane; k < N; k += 32) {
-                const double v = fabs((double)A[(size_t)c.piv[k] * ldA + i]);
-                if (v > best || (v == best && k < bk)) { best = v; bk = k; }
+    CtaCand<T>* cand = static_cast<CtaCand<T>*>(c.cand);
+    T* myrow = A + (size_t)(tid < N ? tid : 0) * ld;
+    bool done = tid >= N;  // row is a pivot row already (or no row)
+    for (int k0 = 0; k0 < N; k0 += CTA_NB) {
+        const int kb = min(CTA_NB, N - k0);
+        const bool act0 = !done;
+        T a[CTA_NB];
+        if (act0) {
+#pragma unroll
+            for (int q = 0; q < CTA_NB / 4; q++) ld4at(myrow + k0 + 4 * q, a + 4 * q);
+        } else {
+#pragma unroll
+            for (int q = 0; q < CTA_NB; q++) a[q] = (T)0;
+        }
+        // 1. panel factorisation, one barrier per column
+#pragma unroll
+        for (int j = 0; j < CTA_NB; j++) {
+            if (j < kb) {
+                // vote: each warp's best row publishes its panel entries and
+                // its packed (key, row) into the step's 64-bit max slot
+                const int g = k0 + j;  // global step: slots rotate mod 3
+                const uint32_t key = done ? 0u : mag_key(a[j]) + 1u;
+                const T myr = nr_rcp(a[j]);  // off the post-vote path
+                const uint32_t wmax = __reduce_max_sync(0xffffffffu, key);
+                const int wl = __ffs(__ballot_sync(0xffffffffu, key == wmax)) - 1;
+                CtaCand<T>* slot = cand + (j & 1) * CTA_WARPS;
+                if (lane == wl && wmax) {
+                    slot[warp].rcp = myr;
+#pragma unroll
+                    for (int q = 0; q < CTA_NB / 4; q++)
+                        st4at(slot[warp].vals + 4 * q, a + 4 * q);
+                    atomicMax(c.best + g % 3, ((unsigned long long)wmax << 32) | (unsigned)(0xffff - tid));
+                }
+                __syncthreads();
+                // the slot read two steps from now is cleared here: its last
+                // readers passed this barrier, its writers have not started
+                if (tid == 0) c.best[(g + 2) % 3] = 0ull;
+                const int pr = 0xffff - (int)(c.best[g % 3] & 0xffffu);
+                const CtaCand<T>& win = slot[pr >> 5];
+                const T ri = win.rcp;
+                if (tid == pr) {
+                    done = true;
+                    c.piv[k0 + j] = pr;
+                    c.rinv[k0 + j] = (double)ri;
+                } else if (!done) {
+                    const T l = a[j] * ri;
+                    a[j] = l;
+#pragma unroll
+                    for (int jj = j + 1; jj < CTA_NB; jj++) a[jj] = fma(-l, win.vals[jj], a[jj]);
+                }
+            }
+        }
+        if (act0) {
+#pragma unroll
+            for (int q = 0; q < CTA_NB / 4; q++) st4at(myrow + k0 + 4 * q, a + 4 * q);
+        }
+        // 2. compaction of the active rows (physical order)
+        const unsigned am = __ballot_sync(0xffffffffu, !done);
+        if (lane == 0) c.misc[warp] = __popc(am);
+        __syncthreads();
+        const int c0 = k0 + CTA_NB;  // first trailing column
+        if (c0 > N) break;           // last panel: b was eliminated in registers
+        if (!done) {
+            int rank = __popc(am & ((1u << lane) - 1u));
+            for (int w = 0; w < warp; w++) rank += c.misc[w];
+            c.act[rank] = tid;
+        }
+        // 3. U12 = L11^-1 A12, one thread per column c0..N
+        int prow[CTA_NB];
+#pragma unroll
+        for (int j = 0; j < CTA_NB; j++) prow[j] = c.piv[k0 + j] * ld;
+        for (int col = c0 + tid; col <= N; col += CTA_THREADS) {
+            T u[CTA_NB];
+#pragma unroll
+            for (int j = 0; j < CTA_NB; j++) u[j] = A[prow[j] + col];
+#pragma unroll
+            for (int i = 0; i < CTA_NB; i++) {
+#pragma unroll
+                for (int j = i + 1; j < CTA_NB; j++) u[j] = fma(-A[prow[j] + k0 + i], u[i], u[j]);
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                const int ok = __shfl_xor_sync(0xffffffffu, bk, o);
-                if (ob > best || (ob == best && ok < bk)) { best = ob; bk = ok; }
-            }
-            if (lane == 0) {
-                if (bk >= N) bk = i;  // all-NaN column: keep the diagonal
-                const int pi = c.piv[i];
-                c.piv[i] = c.piv[bk];
-                c.piv[bk] = pi;
-                c.pstep[c.piv[i]] = i;
-                c.rinv[i] = (double)nr_rcp(A[(size_t)c.piv[i] * ldA + i]);
-            }
-        } else if (STORE_L && i > 0) {
-            // the previous step's multipliers, on physical rows not yet pivot
-            // before step i (pivot step >= i, whatever the swap does)
-            const T ri = (T)c.rinv[i - 1];
-            for (int pr = tid - 32; pr < N; pr += CTA_THREADS - 32)
-                if (c.pstep[pr] >= i) A[(size_t)pr * ldA + (i - 1)] *= ri;
+            for (int j = 1; j < CTA_NB; j++) A[prow[j] + col] = u[j];
         }
         __syncthreads();
-        const T ri = (T)c.rinv[i];
-        const T* prow = A + (size_t)c.piv[i] * ldA;
-        for (int k = i + 1 + ty; k < N; k += 16) {
-            T* row = A + (size_t)c.piv[k] * ldA;
-            const T l = row[i] * ri;
-            for (int t = i + 1 + tx; t <= N; t += 16) row[t] = fma(-l, prow[t], row[t]);
+        // 4. trailing update over act[0..m) x [c0, N], TR x 4 tiles
+        constexpr int TR = 4;
+        const int m = N - c0, n = N + 1 - c0;
+        const int tr = (m + TR - 1) / TR, tc = (n + 3) >> 2;
+        for (int t = tid; t < tr * tc; t += CTA_THREADS) {
+            const int ti = t / tc, col = c0 + 4 * (t - ti * tc);
+            int rows[TR];
+#pragma unroll
+            for (int r = 0; r < TR; r++) {
+                const int rr = TR * ti + r;
+                rows[r] = rr < m ? c.act[rr] * ld : -1;
+            }
+            T acc[TR][4];
+#pragma unroll
+            for (int r = 0; r < TR; r++) {
+                if (rows[r] >= 0) ld4(A + rows[r] + col, acc[r]);
+                else {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[r][q] = (T)0;
+                }
+            }
+#pragma unroll 1  // (full unrolling hoists every load and spills)
+            for (int jc = 0; jc < CTA_NB / 4; jc++) {
+                T u[4][4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) ld4(A + prow[4 * jc + q] + col, u[q]);
+#pragma unroll
+                for (int r = 0; r < TR; r++) {
+                    T l[4] = {(T)0, (T)0, (T)0, (T)0};
+                    if (rows[r] >= 0) ld4(A + rows[r] + k0 + 4 * jc, l);
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+#pragma unroll
+                        for (int cc = 0; cc < 4; cc++) acc[r][cc] = fma(-l[q], u[q][cc], acc[r][cc]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < TR; r++)
+                if (rows[r] >= 0) st4(A + rows[r] + col, acc[r]);
         }
         __syncthreads();
     }
-    // back substitution on warp 0, column-oriented: z[k] = A[piv[k]][N]
-    if (warp == 0) {
-        for (int k = lane; k < N; k += 32) c.z[k] = (double)A[(size_t)c.piv[k] * ldA + N];
-        __syncwarp();
-        for (int i = N - 1; i >= 0; i--) {
-            const double xi = c.z[i] * c.rinv[i];
-            for (int k = lane; k < i; k += 32) c.z[k] = fma(-(double)A[(size_t)c.piv[k] * ldA + i], xi, c.z[k]);
-            if (lane == 0) c.x[i] = xi;
-            __syncwarp();
-        }
-    }
-    __syncthreads();
 }
 
-// Re-solve with stored factors for right-hand side c.r (original order);
-// result in c.x.  Warp 0 only, then a CTA barrier.
-template <typename T>
-__device__ void cta_lu_resolve(const CtaCtx& c, const T* A, int ldA) {
-    const int N = c.N, tid = c.tid;
-    if ((tid >> 5) == 0) {
-        const int lane = tid & 31;
-        for (int k = lane; k < N; k += 32) c.z[k] = c.r[c.piv[k]];
-        __syncwarp();
-        for (int i = 0; i < N; i++) {
-            const double zi = c.z[i];
-            for (int k = i + 1 + lane; k < N; k += 32)
-                c.z[k] = fma(-(double)A[(size_t)c.piv[k] * ldA + i], zi, c.z[k]);
-            __syncwarp();
+// Triangular solves with the factors of cta_lu, on warp 0 alone: lane l
+// owns logical rows l, l+32, ... (z in registers), column sweeps broadcast
+// each finished value by shuffle -- no CTA barrier inside, one at the end.
+//  REFINE = false: z_i = A[piv[i]][N] (already forward-eliminated), solve
+//                  U x = z, write c.x;
+//  REFINE = true:  z_i = c.r[piv[i]], solve L U dx = z, c.x += dx.
+template <typename T, bool REFINE>
+__device__ void cta_solve(const CtaCtx& c, const T* A) {
+    if (c.tid < 32) {
+        const int N = c.N, lane = c.tid, ld = c.ld;
+        constexpr int M = CTA_MAXN / 32;
+        double z[M], xr[M];
+        int rp[M];  // row offsets
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            const int i = lane + 32 * m;
+            const bool in = i < N;
+            const int pr = c.piv[in ? i : 0];
+            rp[m] = pr * ld;
+            z[m] = in ? (REFINE ? c.r[pr] : (double)A[rp[m] + N]) : 0.0;
+            xr[m] = 0.0;
         }
-        for (int i = N - 1; i >= 0; i--) {
-            const double xi = c.z[i] * c.rinv[i];
-            for (int k = lane; k < i; k += 32) c.z[k] = fma(-(double)A[(size_t)c.piv[k] * ldA + i], xi, c.z[k]);
-            if (lane == 0) c.x[i] = xi;
-            __syncwarp();
+        if (REFINE) {
+            // L z = z, unit lower: k = 0 .. N-2
+#pragma unroll
+            for (int b = 0; b < M; b++) {
+                if (32 * b < N) {
+                    const int kend = min(N - 1, 32 * b + 32);
+                    T u[M];  // column k of my rows, loaded one step ahead
+#pragma unroll
+                    for (int m = b; m < M; m++) u[m] = A[rp[m] + 32 * b];
+                    for (int k = 32 * b; k < kend; k++) {
+                        T un[M];
+                        const int kn = k + 1 < kend ? k + 1 : k;
+#pragma unroll
+                        for (int m = b; m < M; m++) un[m] = A[rp[m] + kn];
+                        const double zk = __shfl_sync(0xffffffffu, z[b], k - 32 * b);
+#pragma unroll
+                        for (int m = b; m < M; m++) {
+                            const int i = lane + 32 * m;
+                            if (i > k && i < N) z[m] = fma(-(double)u[m], zk, z[m]);
+                            u[m] = un[m];
+                        }
+                    }
+                }
+            }
+        }
+        // U x = z: k = N-1 .. 0
+#pragma unroll
+        for (int b = M - 1; b >= 0; b--) {
+            if (32 * b < N) {
+                const int ktop = min(N, 32 * b + 32) - 1;
+                T u[M];  // column k of my rows, loaded one step ahead
+#pragma unroll
+                for (int m = 0; m <= b; m++) u[m] = A[rp[m] + ktop];
+                for (int k = ktop; k >= 32 * b; k--) {
+                    T un[M];
+                    const int kn = k > 32 * b ? k - 1 : k;
+#pragma unroll
+                    for (int m = 0; m <= b; m++) un[m] = A[rp[m] + kn];
+                    const double xk = __shfl_sync(0xffffffffu, z[b] * c.rinv[k], k - 32 * b);
+                    xr[b] = (lane == k - 32 * b) ? xk : xr[b];  // kept by its owner, no branch
+#pragma unroll
+                    for (int m = 0; m <= b; m++) {
+                        const int i = lane + 32 * m;
+                        if (i < k) z[m] = fma(-(double)u[m], xk, z[m]);
+                        u[m] = un[m];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            const int i = lane + 32 * m;
+            if (i < N) c.x[i] = REFINE ? c.x[i] + xr[m] : xr[m];
         }
     }
     __syncthreads();
@@ -252,7 +514,7 @@ __device__ void cta_gje_exact(const CtaCtx& c, double h, double* M, double* Inv)
             const int rr = c.inc[e];
             const uint2 q = *reinterpret_cast<const uint2*>(c.sp + 4 * rr);
             const int a = q.x & 0xffff, b = q.x >> 16, cc = q.y & 0xffff, d = q.y >> 16;
-            const xd k = __ldg(c.rates + rr);
+            const xd k = c.rates[rr];
             const xd da = k * xd(c.v[b]), db = k * xd(c.v[a]);
             double* ra = M + (size_t)a * N + j;
             double* rb = M + (size_t)b * N + j;
@@ -326,81 +588,83 @@ __device__ void cta_gje_exact(const CtaCtx& c, double h, double* M, double* Inv)
     __syncthreads();
 }
 
+// One substep of size h on c.v (in place).
 template <int METHOD, int CTRL, int SOLVER>
-__device__ void cta_substep(const CtaCtx& c, double h, void* mat, int ldA, double* gM) {
+__device__ void cta_substep(const CtaCtx& c, double h, void* mat, double* gM) {
     const int N = c.N, tid = c.tid;
+    const bool own = tid < N;
     if (METHOD == WIND_METHOD_RK2) {
-        cta_rhs_jac<false, double>(c, h, nullptr, 0);
-        for (int l = tid; l < N; l += CTA_THREADS) c.v[l] = (xd(c.v[l]) + xd(h) * xd(c.f[l])).v;
+        cta_rhs(c);
+        if (own) c.v[tid] = (xd(c.v[tid]) + xd(h) * xd(c.f[tid])).v;
         __syncthreads();
         return;
     }
     if (SOLVER == WIND_SOLVER_GJE_F64) {
-        cta_rhs_jac<false, double>(c, h, nullptr, 0);
+        cta_rhs(c);
         cta_gje_exact<CTRL>(c, h, gM, gM + (size_t)N * N);
         return;
     }
-    if (SOLVER == WIND_SOLVER_LU_F64) {
-        double* A = static_cast<double*>(mat);
-        cta_rhs_jac<true, double>(c, h, A, ldA);
-        cta_lu_solve<double, false>(c, A, ldA);
-        for (int l = tid; l < N; l += CTA_THREADS) c.v[l] = c.v[l] + h * c.x[l];
-        __syncthreads();
-        return;
+    using T = typename std::conditional<SOLVER == WIND_SOLVER_MIXED, float, double>::type;
+    T* A = static_cast<T*>(mat);
+    cta_build<T>(c, h, A);
+    cta_lu<T>(c, A);
+    cta_solve<T, false>(c, A);
+    if (SOLVER == WIND_SOLVER_MIXED) {
+        // two FP64 refinement steps with the FP32 factors
+        for (int it = 0; it < 2; it++) {
+            if (own) c.r[tid] = c.f[tid] - (c.x[tid] - h * cta_jx(c, tid, c.x));
+            __syncthreads();
+            cta_solve<T, true>(c, A);
+        }
     }
-    float* A = static_cast<float*>(mat);
-    cta_rhs_jac<true, float>(c, h, A, ldA);
-    cta_lu_solve<float, true>(c, A, ldA);
-    // two FP64 refinement steps with the FP32 factors
-    for (int it = 0; it < 2; it++) {
-        for (int l = tid; l < N; l += CTA_THREADS) c.r[l] = c.f[l] - (c.x[l] - h * cta_jx(c, l, c.x));
-        for (int l = tid; l < N; l += CTA_THREADS) c.scr[l] = c.x[l];
-        __syncthreads();
-        cta_lu_resolve<float>(c, A, ldA);
-        for (int l = tid; l < N; l += CTA_THREADS) c.x[l] = c.scr[l] + c.x[l];
-        __syncthreads();
-    }
-    for (int l = tid; l < N; l += CTA_THREADS) c.v[l] = c.v[l] + h * c.x[l];
+    if (own) c.v[tid] = c.v[tid] + h * c.x[tid];
     __syncthreads();
 }
 
 // The persistent CTA loop over one group's systems (blockDim.x must be
-// CTA_THREADS).  `gscratch` holds one matrix slot per block when the layout
-// does not keep the matrix in shared memory (and always for GJE_F64).
+// CTA_THREADS).  `gscratch` holds one slot of `gstride` >=
+// CtaLayout::g_doubles doubles per block (null when the layout needs none).
 template <int METHOD, int CTRL, int SOLVER>
-__device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_raw, double* gscratch, int smem_cap) {
+__device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_raw, double* gscratch,
+                                        size_t gstride, int smem_cap) {
     constexpr int CAP = Cap<METHOD, CTRL>::value;
     const int N = p.n_eq, R = p.n_react, tid = threadIdx.x;
+    const bool own = tid < N;
     const bool lin = p.linear != nullptr;
     const CtaLayout lay(N, R, lin, SOLVER, smem_cap);
     CtaCtx c;
     c.N = N;
     c.R = R;
     c.tid = tid;
+    c.ld = lay.ld;
+    c.cols = lay.cols;
     double* vec = reinterpret_cast<double*>(smem_raw + lay.vec);
     c.v = vec;
     c.f = vec + N;
-    c.y = vec + 2 * N;
-    c.y1 = vec + 3 * N;
-    c.y2 = vec + 4 * N;
-    c.x = vec + 5 * N;
-    c.r = vec + 6 * N;
-    c.z = vec + 7 * N;
-    c.rinv = vec + 8 * N;
-    c.scr = vec + 9 * N;
+    c.x = c.r = c.rinv = c.scr = nullptr;
+    if (SOLVER == WIND_SOLVER_GJE_F64) {
+        c.scr = vec + 2 * N;
+    } else {
+        c.x = vec + 2 * N;
+        c.rinv = vec + 3 * N;
+        if (SOLVER == WIND_SOLVER_MIXED) c.r = vec + 4 * N;
+    }
     c.piv = reinterpret_cast<int*>(smem_raw + lay.piv);
-    c.pstep = c.piv + N;
-    c.misc = c.piv + 2 * N;
-    int* inc_off = reinterpret_cast<int*>(smem_raw + lay.inc_off);
-    uint16_t* inc = reinterpret_cast<uint16_t*>(smem_raw + lay.inc);
+    c.act = reinterpret_cast<int*>(smem_raw + lay.act);
+    c.misc = reinterpret_cast<int*>(smem_raw + lay.misc);
+    c.best = reinterpret_cast<unsigned long long*>(smem_raw + lay.misc + 4 * CTA_WARPS);
+    c.cand = smem_raw + lay.cand;
+    double* gslot = gscratch ? gscratch + (size_t)blockIdx.x * gstride : nullptr;
+    unsigned char* incbase = lay.inc_in_smem ? smem_raw + lay.inc_off
+                                             : reinterpret_cast<unsigned char*>(gslot + lay.g_inc);
+    int* inc_off = reinterpret_cast<int*>(incbase);
+    uint16_t* inc = reinterpret_cast<uint16_t*>(incbase + CtaLayout::a16((N + 1) * 4));
     c.inc_off = inc_off;
     c.inc = inc;
     float* LT = lin ? reinterpret_cast<float*>(smem_raw + lay.lt) : nullptr;
     c.LT = LT;
-    const size_t gsz = CtaLayout::gscratch_doubles(N, SOLVER);
-    double* gM = gscratch ? gscratch + (size_t)blockIdx.x * gsz : nullptr;
-    void* mat = lay.mat_in_smem ? (void*)(smem_raw + lay.mat) : (void*)gM;
-    const int ldA = N + 1;
+    double* gM = gslot;
+    void* mat = lay.mat_in_smem ? (void*)(smem_raw + lay.mat) : (void*)(gslot + lay.g_mat);
     const uint64_t t_start = p.timeout_ns ? global_ns() : 0;
     __shared__ unsigned long long s_ticket;
     __shared__ int s_flag;
@@ -412,6 +676,16 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
         if (s >= p.nsys) break;
         c.rates = p.rates + s * R;
         c.sp = p.species + (s * R) * 4;
+        if (lay.data_in_smem) {
+            double* srt = reinterpret_cast<double*>(smem_raw + lay.rt);
+            uint2* ssp = reinterpret_cast<uint2*>(smem_raw + lay.spc);
+            for (int r = tid; r < R; r += CTA_THREADS) {
+                srt[r] = c.rates[r];
+                ssp[r] = *reinterpret_cast<const uint2*>(c.sp + 4 * r);
+            }
+            c.rates = srt;
+            c.sp = reinterpret_cast<const uint16_t*>(ssp);
+        }
         // validate species indices, then build the per-species incidence lists
         if (tid == 0) s_flag = 0;
         __syncthreads();
@@ -424,14 +698,14 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
         __syncthreads();
         const bool bad = s_flag != 0;
         if (!bad) {
-            for (int j = tid; j < N; j += CTA_THREADS) {
+            if (own) {
                 int cnt = 0;
                 for (int r = 0; r < R; r++) {
                     const uint2 q = *reinterpret_cast<const uint2*>(c.sp + 4 * r);
                     const int a = q.x & 0xffff, b = q.x >> 16, cc = q.y & 0xffff, d = q.y >> 16;
-                    cnt += (a == j || b == j || cc == j || d == j);
+                    cnt += (a == tid || b == tid || cc == tid || d == tid);
                 }
-                inc_off[j + 1] = cnt;
+                inc_off[tid + 1] = cnt;
             }
             __syncthreads();
             if (tid == 0) {
@@ -439,12 +713,12 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
                 for (int j = 0; j < N; j++) inc_off[j + 1] += inc_off[j];
             }
             __syncthreads();
-            for (int j = tid; j < N; j += CTA_THREADS) {
-                int o = inc_off[j];
+            if (own) {
+                int o = inc_off[tid];
                 for (int r = 0; r < R; r++) {
                     const uint2 q = *reinterpret_cast<const uint2*>(c.sp + 4 * r);
                     const int a = q.x & 0xffff, b = q.x >> 16, cc = q.y & 0xffff, d = q.y >> 16;
-                    if (a == j || b == j || cc == j || d == j) inc[o++] = (uint16_t)r;
+                    if (a == tid || b == tid || cc == tid || d == tid) inc[o++] = (uint16_t)r;
                 }
             }
             if (lin) {
@@ -455,7 +729,7 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
                 }
             }
         }
-        for (int l = tid; l < N; l += CTA_THREADS) c.y[l] = p.y[s * N + l];
+        double yl = own ? p.y[s * N + tid] : 0.0, y1l = 0.0, y2l = 0.0;
         __syncthreads();
 
         double tnow = p.tnow;
@@ -466,47 +740,50 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
         int32_t st = bad ? WIND_SYS_BAD_INPUT : WIND_SYS_OK;
         while (!bad && tnow < tend) {
             if (attempts >= p.max_attempts) { st |= WIND_SYS_MAX_ATTEMPTS; break; }
-            if (p.timeout_ns && global_ns() - t_start > p.timeout_ns) { st |= WIND_SYS_TIMEOUT; break; }
+            if (p.timeout_ns) {
+                // thread 0's clock decides for the whole CTA
+                if (__syncthreads_or(tid == 0 && global_ns() - t_start > p.timeout_ns)) {
+                    st |= WIND_SYS_TIMEOUT;
+                    break;
+                }
+            }
             attempts++;
             h = fmin(tend - tnow, h);
             const double t1 = tnow + h;
             for (int pass = 0; pass < 2; pass++) {
                 const int nsub = pass + 1;
-                for (int l = tid; l < N; l += CTA_THREADS) c.v[l] = c.y[l];
+                if (own) c.v[tid] = yl;
                 __syncthreads();
                 // (t1-t0)/nsub, nsub in {1,2}: exact as a multiplication
                 double hs = (t1 - tnow) * (nsub == 1 ? 1.0 : 0.5);
                 double t = tnow;
                 for (int k = 0; k < nsub; k++) {
                     if (CTRL == WIND_CTRL_DEVICE) hs = fmin(t1 - t, hs);
-                    cta_substep<METHOD, CTRL, SOLVER>(c, hs, mat, ldA, gM);
+                    cta_substep<METHOD, CTRL, SOLVER>(c, hs, mat, gM);
                     t += hs;
                 }
-                double* dst = pass == 0 ? c.y1 : c.y2;
-                for (int l = tid; l < N; l += CTA_THREADS) dst[l] = c.v[l];
-                __syncthreads();
+                if (own) {
+                    if (pass == 0) y1l = c.v[tid];
+                    else y2l = c.v[tid];
+                }
             }
-            int e = 0;
-            for (int l = tid; l < N; l += CTA_THREADS)
-                e |= elem_error<METHOD, CTRL>(xd(c.y1[l]), xd(c.y2[l]), p.atol, p.rtol) ? 1 : 0;
+            const int e = own && elem_error<METHOD, CTRL>(xd(y1l), xd(y2l), p.atol, p.rtol) ? 1 : 0;
             const bool err = __syncthreads_or(e) != 0;
             if (err && unsolved < CAP) {
                 unsolved++;
                 h /= 2.0;
             } else {
                 unsolved = 0;
-                for (int l = tid; l < N; l += CTA_THREADS)
-                    c.y[l] = (METHOD == WIND_METHOD_RK2) ? (xd(2.0) * xd(c.y2[l]) - xd(c.y1[l])).v : c.y2[l];
-                if (tnow + h == tnow) { st |= WIND_SYS_STALLED; __syncthreads(); break; }
+                if (own) yl = (METHOD == WIND_METHOD_RK2) ? (xd(2.0) * xd(y2l) - xd(y1l)).v : y2l;
+                if (tnow + h == tnow) { st |= WIND_SYS_STALLED; break; }
                 tnow += h;
                 h = (METHOD == WIND_METHOD_RK2) ? h * 2 : tend - tnow;
             }
-            __syncthreads();
         }
         int nonfinite = 0;
-        for (int l = tid; l < N; l += CTA_THREADS) {
-            if (!finite64(c.y[l])) nonfinite = 1;
-            p.y[s * N + l] = c.y[l];
+        if (own) {
+            if (!finite64(yl)) nonfinite = 1;
+            p.y[s * N + tid] = yl;
         }
         if (__syncthreads_or(nonfinite)) st |= WIND_SYS_NONFINITE;
         if (tid == 0) {
@@ -518,10 +795,20 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
     }
 }
 
+// Two CTAs per SM for the FP32 factors (the 157-species matrix is ~100 KB).
+#ifndef WIND_CTA_MIXED_BLOCKS
+#define WIND_CTA_MIXED_BLOCKS 2
+#endif
+template <int SOLVER>
+struct CtaMinBlocks {
+    static constexpr int value = SOLVER == WIND_SOLVER_MIXED ? WIND_CTA_MIXED_BLOCKS : 1;
+};
+
 template <int METHOD, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(CTA_THREADS) k_cta(const KParams p, double* gscratch, int smem_cap) {
+__global__ void __launch_bounds__(CTA_THREADS, CtaMinBlocks<SOLVER>::value)
+    k_cta(const KParams p, double* gscratch, size_t gstride, int smem_cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, smem_cap);
+    cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, gstride, smem_cap);
 }
 
 }  // namespace wind

@@ -8,7 +8,7 @@
 
 namespace wind {
 
-using CtaFn = void (*)(KParams, double*, int);
+using CtaFn = void (*)(KParams, double*, size_t, int);
 
 template <int METHOD, int CTRL>
 static CtaFn cta_by_solver(int solver) {
@@ -37,6 +37,17 @@ static int smem_optin() {
     return v - 1024;  // room for the kernel's static shared variables
 }
 
+// Dynamic shared memory per block that leaves room for two blocks per SM.
+static int smem_half(CtaFn fn) {
+    int dev = 0, per_sm = 228 * 1024;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaFuncAttributes fa{};
+    size_t stat = 64;
+    if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess) stat = fa.sharedSizeBytes;
+    return (int)((per_sm / 2 - 1024 - (int)stat) & ~127);
+}
+
 static int cta_blocks_per_sm(CtaFn fn, size_t smem) {
     static std::mutex mu;
     static std::vector<std::pair<std::pair<const void*, size_t>, int>> cache;
@@ -54,38 +65,48 @@ static int method_solver(const wind_options& o) {
     return (o.method == WIND_METHOD_RK2) ? WIND_SOLVER_LU_F64 : o.solver;
 }
 
-// Global scratch bytes a CTA launch needs (0 = none) and its grid.
-size_t cta_scratch_bytes(const wind_options& o, const KParams& p, int* grid_out) {
-    const int solver = method_solver(o);
-    const int cap = smem_optin();
-    const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, solver, cap);
-    CtaFn fn = cta_fn(o.method, o.controller, o.solver);
-    const int nb = lay.bytes <= cap ? cta_blocks_per_sm(fn, lay.bytes) : 0;
-    const int64_t resident = (int64_t)(nb > 0 ? nb : 1) * device_sm_count();
-    const int grid = (int)(p.nsys < resident ? p.nsys : resident);
-    if (grid_out) *grid_out = grid;
-    const bool need = (solver == WIND_SOLVER_GJE_F64) || !lay.mat_in_smem;
-    return need ? (size_t)grid * CtaLayout::gscratch_doubles(p.n_eq, solver) * sizeof(double) : 0;
-}
-
-wind_status launch_cta(const wind_options& o, const KParams& p, cudaStream_t stream, double* scratch,
-                       size_t scratch_bytes) {
+// Choose the shared-memory budget (full, or half an SM for the FP32
+// factors), the grid and the per-block global scratch of a CTA launch.
+// With allow_global = false only layouts without global scratch qualify.
+wind_status plan_cta(const wind_options& o, const KParams& p, bool allow_global, CtaPlan* out) {
     if (p.n_eq > CTA_MAXN || p.n_react > 65535) return WIND_ERR_UNSUPPORTED;
     const int solver = method_solver(o);
-    const int cap = smem_optin();
-    const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, solver, cap);
-    if (lay.bytes > cap) return WIND_ERR_UNSUPPORTED;
     CtaFn fn = cta_fn(o.method, o.controller, o.solver);
-    const int nb = cta_blocks_per_sm(fn, lay.bytes);
-    if (nb < 1) return WIND_ERR_UNSUPPORTED;
-    int grid = 0;
-    const size_t need = cta_scratch_bytes(o, p, &grid);
-    if (need > scratch_bytes) return WIND_ERR_NOMEM;
+    int caps[2] = {smem_optin(), 0};
+    int ncap = 1;
+    if (solver == WIND_SOLVER_MIXED && CtaMinBlocks<WIND_SOLVER_MIXED>::value >= 2) caps[ncap++] = smem_half(fn);
+    bool found = false;
+    CtaPlan best{};
+    int best_nb = 0;
+    for (int i = 0; i < ncap; i++) {
+        const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, solver, caps[i]);
+        if (lay.bytes > caps[i]) continue;
+        if (!allow_global && lay.g_doubles > 0) continue;
+        const int nb = cta_blocks_per_sm(fn, lay.bytes);
+        if (nb < 1 || nb <= best_nb) continue;  // ties keep the larger budget
+        const int64_t resident = (int64_t)nb * device_sm_count();
+        best.fn = (const void*)fn;
+        best.smem_cap = caps[i];
+        best.smem_bytes = lay.bytes;
+        best.grid = (int)(p.nsys < resident ? p.nsys : resident);
+        best.gstride = lay.g_doubles;
+        best_nb = nb;
+        found = true;
+    }
+    if (!found) return WIND_ERR_UNSUPPORTED;
+    *out = best;
+    return WIND_OK;
+}
+
+wind_status launch_cta(const CtaPlan& pl, const KParams& p, cudaStream_t stream, double* scratch) {
+    if (pl.gstride && !scratch) return WIND_ERR_ARGUMENT;
+    CtaFn fn = reinterpret_cast<CtaFn>(const_cast<void*>(pl.fn));
     // set for this launch every time (the occupancy cache may come from a
     // launch of the same kernel with another size)
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.bytes) != cudaSuccess)
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.smem_bytes) != cudaSuccess)
         return launch_status("k_cta shared-memory attribute");
-    fn<<<grid, CTA_THREADS, lay.bytes, stream>>>(p, need ? scratch : nullptr, cap);
+    fn<<<pl.grid, CTA_THREADS, pl.smem_bytes, stream>>>(p, pl.gstride ? scratch : nullptr, pl.gstride,
+                                                        pl.smem_cap);
     g_launches++;
     return launch_status("k_cta launch");
 }

@@ -10,7 +10,7 @@
 
 namespace wind {
 
-using MixedFn = void (*)(const KParams*, const int*, int, double*, int);
+using MixedFn = void (*)(const KParams*, const int*, int, double*, size_t, int);
 
 template <int METHOD, int CTRL>
 static MixedFn mixed_by_solver(int solver) {
@@ -48,8 +48,7 @@ wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, 
         if (p.n_eq > 32) {
             const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, solver, cap);
             smem = std::max(smem, (size_t)lay.bytes);
-            if (solver == WIND_SOLVER_GJE_F64 || !lay.mat_in_smem)
-                gslot = std::max(gslot, CtaLayout::gscratch_doubles(p.n_eq, solver));
+            gslot = std::max(gslot, lay.g_doubles);
         } else {
             const int nm = nmax_of(p.n_eq);
             smem = std::max(smem, (size_t)(MIXED_THREADS / nm) * TeamLayout(nm, p.n_react, p.linear != nullptr, solver).bytes);
@@ -89,7 +88,7 @@ wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, 
     if (st == WIND_OK) {
         fn<<<grid, MIXED_THREADS, smem, stream>>>(reinterpret_cast<const KParams*>(dparams),
                                                   reinterpret_cast<const int*>(dparams + pbytes),
-                                                  (int)ps.size(), gscratch, cap);
+                                                  (int)ps.size(), gscratch, gslot, cap);
         g_launches++;
         st = launch_status("k_mixed launch");
     }

@@ -24,6 +24,10 @@
 namespace wind {
 
 constexpr int LANE_THREADS = 128;
+// Minimum resident blocks per SM the compiler must allow (register cap).
+#ifndef WIND_LANE_MIN_BLOCKS
+#define WIND_LANE_MIN_BLOCKS 1
+#endif
 
 // One SIE or explicit-Euler substep of length h, in place on y.
 template <class Net, int METHOD, int CTRL, int SOLVER>
@@ -191,7 +195,7 @@ __device__ __forceinline__ unsigned team_mask_of(int j, int nact, int wmax) {
 // others start as helpers, which spreads a small batch over many warps
 // (opw = 32 / initial lanes per system).
 template <class Net, int METHOD, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(LANE_THREADS) k_lane(const KParams p, const int opw) {
+__global__ void __launch_bounds__(LANE_THREADS, WIND_LANE_MIN_BLOCKS) k_lane(const KParams p, const int opw) {
     constexpr int N = Net::N;
     constexpr int NC = Net::NC;
     constexpr int CAP = Cap<METHOD, CTRL>::value;

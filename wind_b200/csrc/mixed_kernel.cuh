@@ -20,12 +20,12 @@ constexpr int MIXED_THREADS = CTA_THREADS;
 template <int METHOD, int CTRL, int SOLVER>
 __global__ void __launch_bounds__(MIXED_THREADS, 1)
     k_mixed(const KParams* __restrict__ groups, const int* __restrict__ order, int ngroups,
-            double* gscratch, int smem_cap) {
+            double* gscratch, size_t gstride, int smem_cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     for (int gi = 0; gi < ngroups; gi++) {
         const KParams p = groups[order[gi]];
         if (p.nsys > 0) {
-            if (p.n_eq > 32) cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, smem_cap);
+            if (p.n_eq > 32) cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, gstride, smem_cap);
             else if (p.n_eq > 16) team_run<32, METHOD, CTRL, SOLVER>(p, smem_raw);
             else if (p.n_eq > 8) team_run<16, METHOD, CTRL, SOLVER>(p, smem_raw);
             else team_run<8, METHOD, CTRL, SOLVER>(p, smem_raw);

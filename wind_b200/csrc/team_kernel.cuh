@@ -608,7 +608,11 @@ __device__ __forceinline__ void team_run(const KParams& p, unsigned char* smem_r
         int32_t st = bad_idx ? WIND_SYS_BAD_INPUT : WIND_SYS_OK;
         while (!bad_idx && tnow < tend) {
             if (attempts >= p.max_attempts) { st |= WIND_SYS_MAX_ATTEMPTS; break; }
-            if (p.timeout_ns && global_ns() - t_start > p.timeout_ns) { st |= WIND_SYS_TIMEOUT; break; }
+            if (p.timeout_ns) {
+                // the leader's clock decides for the whole team
+                const int late = global_ns() - t_start > p.timeout_ns;
+                if (__shfl_sync(c.mask, late, c.leader)) { st |= WIND_SYS_TIMEOUT; break; }
+            }
             attempts++;
             h = fmin(tend - tnow, h);
             // full step into y1

@@ -24,7 +24,8 @@ from . import _capi
 from .networks import Network
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBDIR = os.path.join(HERE, "lib")
+# WIND_LIBDIR selects another build of the libraries (e.g. an experiment)
+LIBDIR = os.environ.get("WIND_LIBDIR", os.path.join(HERE, "lib"))
 
 _lib = None
 
