@@ -76,9 +76,12 @@ enum { WIND_CTRL_DEVICE = 0, WIND_CTRL_GOLD = 1 };
  *          (cuda/c_baseline/linear_algebra/gje_gold.c:5-144,
  *           cuda/linear_algebra/gauss_jordan_elimination.cu:15-212).
  * LU_F64:  partial-pivot LU solve in FP64.
- * MIXED:   FP32 partial-pivot LU factor, FP64 residual, FP64 iterative
- *          refinement; falls back to LU_F64 for a system whose refinement
- *          does not converge (flag WIND_SYS_REFINE_FALLBACK). */
+ * MIXED:   FP32 LU factors, FP64 residual from the network, FP64 iterative
+ *          refinement.  N <= 32: partial pivoting.  32 < N: no pivoting
+ *          (the reference's elimination order); a substep whose refinement
+ *          does not converge (last correction above 1e-6 of max |x|) is
+ *          redone with partial pivoting and the system is flagged
+ *          WIND_SYS_REFINE_FALLBACK. */
 enum { WIND_SOLVER_GJE_F64 = 0, WIND_SOLVER_LU_F64 = 1, WIND_SOLVER_MIXED = 2 };
 
 /* Network kinds: the ode_system plug-ins (cuda/include/device.h:1-13,

@@ -48,6 +48,7 @@ constexpr int CTA_THREADS = 256;
 constexpr int CTA_WARPS = CTA_THREADS / 32;
 constexpr int CTA_MAXN = 256;
 constexpr int CTA_NB = 16;  // LU panel width
+constexpr int CTA_CONV = 14; // misc[] slot: refinement converged (0/1)
 
 // A warp's pivot candidate for one panel column.
 template <typename T>
@@ -285,6 +286,72 @@ __device__ __forceinline__ double cta_jx(const CtaCtx& c, int j, const double* x
     return acc;
 }
 
+// U12 = L11^-1 A12 for the 16 pivot rows of the panel at k0 (row offsets
+// prow[]), one thread per column c0..N.
+template <typename T>
+__device__ __forceinline__ void cta_u12(const CtaCtx& c, T* A, int k0, const int (&prow)[CTA_NB]) {
+    const int N = c.N;
+    for (int col = k0 + CTA_NB + c.tid; col <= N; col += CTA_THREADS) {
+        T u[CTA_NB];
+#pragma unroll
+        for (int j = 0; j < CTA_NB; j++) u[j] = A[prow[j] + col];
+#pragma unroll
+        for (int i = 0; i < CTA_NB; i++) {
+#pragma unroll
+            for (int j = i + 1; j < CTA_NB; j++) u[j] = fma(-A[prow[j] + k0 + i], u[i], u[j]);
+        }
+#pragma unroll
+        for (int j = 1; j < CTA_NB; j++) A[prow[j] + col] = u[j];
+    }
+}
+
+// Trailing update A22 -= L21 U12 of the panel at k0: the active rows
+// (act[0..m) with pivoting, rows c0..N-1 in order without) times columns
+// c0..N, 4x4 register tiles with 16-byte vectors.
+template <typename T, bool NATURAL>
+__device__ __forceinline__ void cta_trailing(const CtaCtx& c, T* A, int k0, const int (&prow)[CTA_NB]) {
+    constexpr int TR = 4;
+    const int N = c.N, ld = c.ld, c0 = k0 + CTA_NB;
+    const int m = N - c0, n = N + 1 - c0;
+    const int tr = (m + TR - 1) / TR, tc = (n + 3) >> 2;
+    for (int t = c.tid; t < tr * tc; t += CTA_THREADS) {
+        const int ti = t / tc, col = c0 + 4 * (t - ti * tc);
+        int rows[TR];
+#pragma unroll
+        for (int r = 0; r < TR; r++) {
+            const int rr = TR * ti + r;
+            rows[r] = rr < m ? (NATURAL ? c0 + rr : c.act[rr]) * ld : -1;
+        }
+        T acc[TR][4];
+#pragma unroll
+        for (int r = 0; r < TR; r++) {
+            if (rows[r] >= 0) ld4(A + rows[r] + col, acc[r]);
+            else {
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[r][q] = (T)0;
+            }
+        }
+#pragma unroll 1  // (full unrolling hoists every load and spills)
+        for (int jc = 0; jc < CTA_NB / 4; jc++) {
+            T u[4][4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) ld4(A + prow[4 * jc + q] + col, u[q]);
+#pragma unroll
+            for (int r = 0; r < TR; r++) {
+                T l[4] = {(T)0, (T)0, (T)0, (T)0};
+                if (rows[r] >= 0) ld4(A + rows[r] + k0 + 4 * jc, l);
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+#pragma unroll
+                    for (int cc = 0; cc < 4; cc++) acc[r][cc] = fma(-l[q], u[q][cc], acc[r][cc]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < TR; r++)
+            if (rows[r] >= 0) st4(A + rows[r] + col, acc[r]);
+    }
+}
+
 // Blocked right-looking LU with partial pivoting of [A | b] in place (see
 // the file comment).  On return: c.piv[i] = physical row of logical row i,
 // c.rinv[i] = 1/U_ii, the multipliers below the pivots, U above, and
@@ -364,59 +431,81 @@ __device__ void cta_lu(const CtaCtx& c, T* A) {
         int prow[CTA_NB];
 #pragma unroll
         for (int j = 0; j < CTA_NB; j++) prow[j] = c.piv[k0 + j] * ld;
-        for (int col = c0 + tid; col <= N; col += CTA_THREADS) {
-            T u[CTA_NB];
+        cta_u12<T>(c, A, k0, prow);
+        __syncthreads();
+        // 4. trailing update over act[0..m) x [c0, N]
+        cta_trailing<T, false>(c, A, k0, prow);
+        __syncthreads();
+    }
+}
+
+// LU without pivoting (the elimination order of the reference's
+// Gauss-Jordan inverse), for the FP32 factors of MIXED, whose refinement
+// checks convergence and falls back to cta_lu.  Per panel at k0: warp 0
+// factors the 16 x 16 diagonal block with shuffles; every row below then
+// computes its own multipliers in registers from U11 while the U12 columns
+// are formed; then the trailing update -- three barriers per panel against
+// nineteen with the pivot vote.
+template <typename T>
+__device__ void cta_lu_nopiv(const CtaCtx& c, T* A) {
+    const int N = c.N, tid = c.tid, ld = c.ld;
+    if (tid < N) c.piv[tid] = tid;
+    for (int k0 = 0; k0 < N; k0 += CTA_NB) {
+        const int kb = min(CTA_NB, N - k0);
+        if (tid < 32) {
+            const int lane = tid;
+            const bool mine = lane < kb;
+            T* row = A + (size_t)(k0 + (mine ? lane : 0)) * ld + k0;
+            T a[CTA_NB];
 #pragma unroll
-            for (int j = 0; j < CTA_NB; j++) u[j] = A[prow[j] + col];
-#pragma unroll
-            for (int i = 0; i < CTA_NB; i++) {
-#pragma unroll
-                for (int j = i + 1; j < CTA_NB; j++) u[j] = fma(-A[prow[j] + k0 + i], u[i], u[j]);
+            for (int q = 0; q < CTA_NB / 4; q++) {
+                if (mine) ld4at(row + 4 * q, a + 4 * q);
+                else a[4 * q] = a[4 * q + 1] = a[4 * q + 2] = a[4 * q + 3] = (T)0;
             }
 #pragma unroll
-            for (int j = 1; j < CTA_NB; j++) A[prow[j] + col] = u[j];
+            for (int j = 0; j < CTA_NB; j++) {
+                if (j < kb) {
+                    const T ri = __shfl_sync(0xffffffffu, nr_rcp(a[j]), j);
+                    if (lane == j) c.rinv[k0 + j] = (double)ri;
+                    const bool upd = mine && lane > j;
+                    const T l = a[j] * ri;
+                    if (upd) a[j] = l;
+#pragma unroll
+                    for (int jj = j + 1; jj < CTA_NB; jj++) {
+                        const T pv = __shfl_sync(0xffffffffu, a[jj], j);
+                        if (upd) a[jj] = fma(-l, pv, a[jj]);
+                    }
+                }
+            }
+            if (mine) {
+#pragma unroll
+                for (int q = 0; q < CTA_NB / 4; q++) st4at(row + 4 * q, a + 4 * q);
+            }
         }
         __syncthreads();
-        // 4. trailing update over act[0..m) x [c0, N], TR x 4 tiles
-        constexpr int TR = 4;
-        const int m = N - c0, n = N + 1 - c0;
-        const int tr = (m + TR - 1) / TR, tc = (n + 3) >> 2;
-        for (int t = tid; t < tr * tc; t += CTA_THREADS) {
-            const int ti = t / tc, col = c0 + 4 * (t - ti * tc);
-            int rows[TR];
+        const int c0 = k0 + CTA_NB;
+        if (c0 > N) break;  // last panel: b was eliminated with the block
+        int prow[CTA_NB];
 #pragma unroll
-            for (int r = 0; r < TR; r++) {
-                const int rr = TR * ti + r;
-                rows[r] = rr < m ? c.act[rr] * ld : -1;
-            }
-            T acc[TR][4];
+        for (int j = 0; j < CTA_NB; j++) prow[j] = (k0 + j) * ld;
+        if (tid >= c0 && tid < N) {
+            T* row = A + (size_t)tid * ld + k0;
+            T a[CTA_NB];
 #pragma unroll
-            for (int r = 0; r < TR; r++) {
-                if (rows[r] >= 0) ld4(A + rows[r] + col, acc[r]);
-                else {
+            for (int q = 0; q < CTA_NB / 4; q++) ld4at(row + 4 * q, a + 4 * q);
 #pragma unroll
-                    for (int q = 0; q < 4; q++) acc[r][q] = (T)0;
-                }
-            }
-#pragma unroll 1  // (full unrolling hoists every load and spills)
-            for (int jc = 0; jc < CTA_NB / 4; jc++) {
-                T u[4][4];
+            for (int j = 0; j < CTA_NB; j++) {
+                const T l = a[j] * (T)c.rinv[k0 + j];
+                a[j] = l;
 #pragma unroll
-                for (int q = 0; q < 4; q++) ld4(A + prow[4 * jc + q] + col, u[q]);
-#pragma unroll
-                for (int r = 0; r < TR; r++) {
-                    T l[4] = {(T)0, (T)0, (T)0, (T)0};
-                    if (rows[r] >= 0) ld4(A + rows[r] + k0 + 4 * jc, l);
-#pragma unroll
-                    for (int q = 0; q < 4; q++)
-#pragma unroll
-                        for (int cc = 0; cc < 4; cc++) acc[r][cc] = fma(-l[q], u[q][cc], acc[r][cc]);
-                }
+                for (int jj = j + 1; jj < CTA_NB; jj++) a[jj] = fma(-l, A[prow[j] + k0 + jj], a[jj]);
             }
 #pragma unroll
-            for (int r = 0; r < TR; r++)
-                if (rows[r] >= 0) st4(A + rows[r] + col, acc[r]);
+            for (int q = 0; q < CTA_NB / 4; q++) st4at(row + 4 * q, a + 4 * q);
         }
+        cta_u12<T>(c, A, k0, prow);
+        __syncthreads();
+        cta_trailing<T, true>(c, A, k0, prow);
         __syncthreads();
     }
 }
@@ -492,10 +581,23 @@ __device__ void cta_solve(const CtaCtx& c, const T* A) {
                 }
             }
         }
+        double dxm = 0.0, xm = 0.0;
 #pragma unroll
         for (int m = 0; m < M; m++) {
             const int i = lane + 32 * m;
-            if (i < N) c.x[i] = REFINE ? c.x[i] + xr[m] : xr[m];
+            if (i < N) {
+                const double xn = REFINE ? c.x[i] + xr[m] : xr[m];
+                c.x[i] = xn;
+                dxm = fmax(dxm, fabs(xr[m]));
+                xm = fmax(xm, fabs(xn));
+                if (!(xr[m] == xr[m])) dxm = xr[m];  // NaN stays visible
+            }
+        }
+        if (REFINE) {
+            // converged: the last correction is below 1e-6 of max |x|
+            int ok = dxm <= 1e-6 * xm;
+            ok = __all_sync(0xffffffffu, ok);
+            if (lane == 0) c.misc[CTA_CONV] = ok;
         }
     }
     __syncthreads();
@@ -588,37 +690,50 @@ __device__ void cta_gje_exact(const CtaCtx& c, double h, double* M, double* Inv)
     __syncthreads();
 }
 
-// One substep of size h on c.v (in place).
+// One substep of size h on c.v (in place).  Returns true when the MIXED
+// solve had to be redone with pivoting (uniform across the CTA).
 template <int METHOD, int CTRL, int SOLVER>
-__device__ void cta_substep(const CtaCtx& c, double h, void* mat, double* gM) {
+__device__ bool cta_substep(const CtaCtx& c, double h, void* mat, double* gM) {
     const int N = c.N, tid = c.tid;
     const bool own = tid < N;
     if (METHOD == WIND_METHOD_RK2) {
         cta_rhs(c);
         if (own) c.v[tid] = (xd(c.v[tid]) + xd(h) * xd(c.f[tid])).v;
         __syncthreads();
-        return;
+        return false;
     }
     if (SOLVER == WIND_SOLVER_GJE_F64) {
         cta_rhs(c);
         cta_gje_exact<CTRL>(c, h, gM, gM + (size_t)N * N);
-        return;
+        return false;
     }
     using T = typename std::conditional<SOLVER == WIND_SOLVER_MIXED, float, double>::type;
     T* A = static_cast<T*>(mat);
+    bool fell = false;
     cta_build<T>(c, h, A);
-    cta_lu<T>(c, A);
-    cta_solve<T, false>(c, A);
     if (SOLVER == WIND_SOLVER_MIXED) {
-        // two FP64 refinement steps with the FP32 factors
-        for (int it = 0; it < 2; it++) {
-            if (own) c.r[tid] = c.f[tid] - (c.x[tid] - h * cta_jx(c, tid, c.x));
-            __syncthreads();
-            cta_solve<T, true>(c, A);
+        // unpivoted FP32 factors and two FP64 refinement steps; if the last
+        // correction is not small, redo the substep with partial pivoting
+        for (int pass = 0; pass < 2; pass++) {
+            if (pass == 0) cta_lu_nopiv<T>(c, A);
+            else cta_lu<T>(c, A);
+            cta_solve<T, false>(c, A);
+            for (int it = 0; it < 2; it++) {
+                if (own) c.r[tid] = c.f[tid] - (c.x[tid] - h * cta_jx(c, tid, c.x));
+                __syncthreads();
+                cta_solve<T, true>(c, A);
+            }
+            if (c.misc[CTA_CONV] || pass == 1) break;
+            fell = true;
+            cta_build<T>(c, h, A);
         }
+    } else {
+        cta_lu<T>(c, A);
+        cta_solve<T, false>(c, A);
     }
     if (own) c.v[tid] = c.v[tid] + h * c.x[tid];
     __syncthreads();
+    return fell;
 }
 
 // The persistent CTA loop over one group's systems (blockDim.x must be
@@ -759,7 +874,7 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
                 double t = tnow;
                 for (int k = 0; k < nsub; k++) {
                     if (CTRL == WIND_CTRL_DEVICE) hs = fmin(t1 - t, hs);
-                    cta_substep<METHOD, CTRL, SOLVER>(c, hs, mat, gM);
+                    if (cta_substep<METHOD, CTRL, SOLVER>(c, hs, mat, gM)) st |= WIND_SYS_REFINE_FALLBACK;
                     t += hs;
                 }
                 if (own) {
