@@ -24,10 +24,16 @@
 namespace wind {
 
 constexpr int LANE_THREADS = 128;
-// Minimum resident blocks per SM the compiler must allow (register cap).
-#ifndef WIND_LANE_MIN_BLOCKS
-#define WIND_LANE_MIN_BLOCKS 1
-#endif
+// Minimum resident blocks per SM the compiler must plan registers for.  The
+// LU solver runs faster capped at 128 registers (4 blocks of 128 threads per
+// SM: 51-52 ms against 63-64 ms per 65,536-cell Katz96 call, measured back
+// to back on one B200, despite ~230 bytes of spills); the Gauss-Jordan path
+// loses under the same cap (600 -> 678 ms) and the mixed path was not
+// measured capped, so both keep the uncapped allocation.
+template <int SOLVER>
+struct LaneMinBlocks {
+    static constexpr int value = SOLVER == WIND_SOLVER_LU_F64 ? 4 : 1;
+};
 
 // One SIE or explicit-Euler substep of length h, in place on y.
 template <class Net, int METHOD, int CTRL, int SOLVER>
@@ -195,7 +201,7 @@ __device__ __forceinline__ unsigned team_mask_of(int j, int nact, int wmax) {
 // others start as helpers, which spreads a small batch over many warps
 // (opw = 32 / initial lanes per system).
 template <class Net, int METHOD, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(LANE_THREADS, WIND_LANE_MIN_BLOCKS) k_lane(const KParams p, const int opw) {
+__global__ void __launch_bounds__(LANE_THREADS, LaneMinBlocks<SOLVER>::value) k_lane(const KParams p, const int opw) {
     constexpr int N = Net::N;
     constexpr int NC = Net::NC;
     constexpr int CAP = Cap<METHOD, CTRL>::value;
