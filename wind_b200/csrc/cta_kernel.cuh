@@ -15,10 +15,11 @@
 //  LU_F64   blocked right-looking LU with partial pivoting, FP64, on the
 //           matrix [A | b] in shared memory (global scratch when it does not
 //           fit), followed by blocked triangular solves;
-//  MIXED    the same LU with FP32 factors, FP64 residual r = f - (x - h J x)
-//           evaluated from the reactions (no FP64 matrix), two FP64
-//           refinement steps with the FP32 factors.  Its footprint lets two
-//           CTAs share an SM at N = 157.
+//  MIXED    FP32 factors without pivoting, FP64 residual r = f - (x - h J x)
+//           evaluated from the reactions (no FP64 matrix), FP64 refinement
+//           until the correction is below 1e-6 of max |x| (at most two
+//           steps), else the substep is redone with partial pivoting.  Its
+//           footprint lets two CTAs share an SM at N = 157.
 //
 // Blocked LU (panel width CTA_NB = 16).  Rows never move: logical row i is
 // physical row piv[i].  For each panel:
@@ -712,8 +713,9 @@ __device__ bool cta_substep(const CtaCtx& c, double h, void* mat, double* gM) {
     bool fell = false;
     cta_build<T>(c, h, A);
     if (SOLVER == WIND_SOLVER_MIXED) {
-        // unpivoted FP32 factors and two FP64 refinement steps; if the last
-        // correction is not small, redo the substep with partial pivoting
+        // unpivoted FP32 factors and up to two FP64 refinement steps (the
+        // second only when the first correction is not yet small); if the
+        // last correction is not small, redo the substep with pivoting
         for (int pass = 0; pass < 2; pass++) {
             if (pass == 0) cta_lu_nopiv<T>(c, A);
             else cta_lu<T>(c, A);
@@ -722,6 +724,7 @@ __device__ bool cta_substep(const CtaCtx& c, double h, void* mat, double* gM) {
                 if (own) c.r[tid] = c.f[tid] - (c.x[tid] - h * cta_jx(c, tid, c.x));
                 __syncthreads();
                 cta_solve<T, true>(c, A);
+                if (c.misc[CTA_CONV]) break;
             }
             if (c.misc[CTA_CONV] || pass == 1) break;
             fell = true;
