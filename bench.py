@@ -477,8 +477,15 @@ def main():
     alg_bytes = net.nsys * (16 * N) + net.nbytes()
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    # DRAM bytes per launch from the committed ncu capture of the Katz96
+    # kernel (profiles/k_lane_katz96_lu_16384cells.md: 2.000 MB read + 0.239
+    # MB written for 16,384 cells, i.e. 136.7 B per cell; every cell's state
+    # and constants cross HBM once, so it scales with the cell count)
+    traffic = 136.7 * net.nsys if net.kind == W.NET_KATZ96 else None
     roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": None,
+            "frac": achieved / peak, "traffic": traffic,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, 16,384-cell "
+                               "capture scaled by cells" if traffic is not None else None),
             "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
             "flops_per_substep": flops_per_substep(wl, args.method), "substeps_per_launch": nsub,
             "hbm": {"alg_bytes_per_launch": alg_bytes,
