@@ -220,90 +220,6 @@ __device__ __forceinline__ unsigned pivot_key(double a, int lane_in_team, bool a
     return (__float_as_uint(m) & ~31u) | (31u - (unsigned)lane_in_team);
 }
 
-// Partial-pivot LU solve (I - hJ) x = f with rows one per lane.  T is the
-// factor type (double or float); the right-hand side is carried in FP64.
-// On return c.x holds x.  Keeps the factors in registers for refinement.
-template <int NMAX, typename T>
-struct TeamLU {
-    T Ar[NMAX];
-    T rinv;
-    int piv[NMAX];
-    int mystep;
-
-    __device__ __forceinline__ void factor_solve(const TeamCtx<NMAX>& c, double h) {
-        const int l = c.l, N = c.N;
-#pragma unroll
-        for (int t = 0; t < NMAX; t++) {
-            const double j = (l < N && t < N) ? c.Js[t * NMAX + l] : 0.0;
-            Ar[t] = (T)((t == l ? 1.0 : 0.0) - h * j);
-        }
-        double b = (l < N) ? c.f[l] : 0.0;
-        mystep = (l < N) ? NMAX : -1;  // NMAX = not yet pivot
-        rinv = (T)0;
-#pragma unroll
-        for (int i = 0; i < NMAX; i++) {
-            piv[i] = 0;
-            if (i < N) {
-                const unsigned key = pivot_key((double)Ar[i], l, mystep == NMAX);
-                const unsigned kmax = __reduce_max_sync(c.mask, key);
-                const int p = 31 - (int)(kmax & 31u);
-                piv[i] = p;
-                double* buf = c.bc + (i & 1) * (2 * NMAX + 4);
-                if (l == p) {
-                    mystep = i;
-                    rinv = nr_rcp(Ar[i]);
-#pragma unroll
-                    for (int t = 0; t < NMAX; t++) buf[t] = (double)Ar[t];
-                    buf[2 * NMAX] = (double)rinv;
-                    buf[2 * NMAX + 1] = b;
-                }
-                team_sync(c.mask);
-                if (mystep == NMAX) {
-                    const T lk = Ar[i] * (T)buf[2 * NMAX];
-                    Ar[i] = lk;
-#pragma unroll
-                    for (int t = i + 1; t < NMAX; t++) Ar[t] = fma(-lk, (T)buf[t], Ar[t]);
-                    b = fma(-(double)lk, buf[2 * NMAX + 1], b);
-                }
-            }
-        }
-        back_substitute(c, b);
-    }
-
-    // z (held by pivot lanes in b) -> x, written to c.x
-    __device__ __forceinline__ void back_substitute(const TeamCtx<NMAX>& c, double b) {
-        const int l = c.l, N = c.N;
-        double xl = 0.0;
-#pragma unroll
-        for (int i = NMAX - 1; i >= 0; i--) {
-            if (i < N) {
-                const int p = piv[i];
-                double xi = (l == p) ? b * (double)rinv : 0.0;
-                xi = __shfl_sync(c.mask, xi, c.leader + p);
-                if (mystep < i) b = fma(-(double)Ar[i], xi, b);
-                if (l == i) xl = xi;
-            }
-        }
-        if (l < N) c.x[l] = xl;
-        team_sync(c.mask);
-    }
-
-    // Solve with the stored factors for rhs r_l (held by lane l in original
-    // row order).  Result in c.x.
-    __device__ __forceinline__ void resolve(const TeamCtx<NMAX>& c, double r) {
-        const int N = c.N;
-#pragma unroll
-        for (int i = 0; i < NMAX; i++) {
-            if (i < N) {
-                const int p = piv[i];
-                const double rp = __shfl_sync(c.mask, r, c.leader + p);
-                if (mystep > i) r = fma(-(double)Ar[i], rp, r);
-            }
-        }
-        back_substitute(c, r);
-    }
-};
-
 // Row pitch of the shared LU matrix, in elements: a multiple of 16 bytes so
 // rows can be read as 16-byte vectors (2 doubles / 4 floats), and 16 bytes
 // more than a multiple of 128 so the 8 lanes of a quarter warp hit distinct
