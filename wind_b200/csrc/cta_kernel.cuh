@@ -22,17 +22,21 @@
 //           footprint lets two CTAs share an SM at N = 157.
 //
 // Blocked LU (panel width CTA_NB = 16).  Rows never move: logical row i is
-// physical row piv[i].  For each panel:
+// physical row piv[i].  For each panel (cta_lu, partial pivoting):
 //  1. panel factorisation: thread p holds the 16 panel entries of physical
 //     row p in registers.  Per column one CTA barrier: each warp's best
-//     candidate (max |a| by a __reduce_max_sync key, lowest row on ties)
-//     publishes its row's panel entries in a per-warp slot (double-
-//     buffered), every thread then picks the best slot and eliminates its
-//     own row in registers;
+//     candidate (max |a| by a __reduce_max_sync key) publishes its row's
+//     panel entries and reciprocal pivot in a per-warp slot (double-
+//     buffered) and its packed (key, row) in a 64-bit atomicMax vote (lowest
+//     row on ties); after the barrier every thread reads the winner and
+//     eliminates its own row in registers;
 //  2. the still-active rows are compacted into act[] (warp ballots);
 //  3. U12 = L11^-1 A12 for the 16 pivot rows, one thread per column;
 //  4. trailing update A22 -= L21 U12 over act[] x columns, 4x4 register
 //     tiles with 16-byte shared-memory vectors.
+// The MIXED solver factors without pivoting (cta_lu_nopiv): warp 0 factors
+// the 16x16 diagonal block with shuffles, the rows below form their own
+// multipliers, then steps 3 and 4 -- three barriers per panel.
 // The right-hand side is column N, so the forward elimination comes with the
 // factorisation; the row stride is padded so that rows start 16 bytes apart
 // in the bank space (no conflicts when 32 rows are read at one column).
@@ -51,14 +55,15 @@ constexpr int CTA_MAXN = 256;
 constexpr int CTA_NB = 16;  // LU panel width
 constexpr int CTA_CONV = 14; // misc[] slot: refinement converged (0/1)
 
-// A warp's pivot candidate for one panel column.
+// A warp's pivot candidate for one panel column: its best row's panel
+// entries and the reciprocal of the entry in the column.
 template <typename T>
 struct CtaCand {
-    uint32_t key;
-    int row;
     T rcp;                      // 1 / vals[column] (computed before the vote)
     alignas(16) T vals[CTA_NB];
 };
+static_assert(sizeof(CtaCand<float>) == 16 + CTA_NB * 4, "candidate slot size");
+static_assert(sizeof(CtaCand<double>) == 16 + CTA_NB * 8, "candidate slot size");
 
 // Shared-memory and global-scratch layout of one CTA, computed on the host
 // and the device alike.  Shared memory holds, in order of priority, the
