@@ -79,8 +79,9 @@ enum { WIND_CTRL_DEVICE = 0, WIND_CTRL_GOLD = 1 };
  * MIXED:   FP32 LU factors, FP64 residual from the network, FP64 iterative
  *          refinement.  N <= 32: partial pivoting.  32 < N: no pivoting
  *          (the reference's elimination order); a substep whose refinement
- *          does not converge (last correction above 1e-6 of max |x|) is
- *          redone with partial pivoting and the system is flagged
+ *          does not converge (after two steps, a correction above 1e-6 of
+ *          the largest |x| in its 32-row slice i, i+32, ...) is redone with
+ *          partial pivoting and the system is flagged
  *          WIND_SYS_REFINE_FALLBACK. */
 enum { WIND_SOLVER_GJE_F64 = 0, WIND_SOLVER_LU_F64 = 1, WIND_SOLVER_MIXED = 2 };
 

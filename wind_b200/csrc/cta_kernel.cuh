@@ -17,9 +17,9 @@
 //           fit), followed by blocked triangular solves;
 //  MIXED    FP32 factors without pivoting, FP64 residual r = f - (x - h J x)
 //           evaluated from the reactions (no FP64 matrix), FP64 refinement
-//           until the correction is below 1e-6 of max |x| (at most two
-//           steps), else the substep is redone with partial pivoting.  Its
-//           footprint lets two CTAs share an SM at N = 157.
+//           until the correction is below 1e-6 of |x| (per 32-row slice; at
+//           most two steps), else the substep is redone with partial
+//           pivoting.  Its footprint lets two CTAs share an SM at N = 157.
 //
 // Blocked LU (panel width CTA_NB = 16).  Rows never move: logical row i is
 // physical row piv[i].  For each panel (cta_lu, partial pivoting):
@@ -600,7 +600,9 @@ __device__ void cta_solve(const CtaCtx& c, const T* A) {
             }
         }
         if (REFINE) {
-            // converged: the last correction is below 1e-6 of max |x|
+            // converged: on every lane the last correction is below 1e-6 of
+            // the largest |x| among the lane's rows (l, l+32, ...) -- at
+            // least as strict as the same test over all rows
             int ok = dxm <= 1e-6 * xm;
             ok = __all_sync(0xffffffffu, ok);
             if (lane == 0) c.misc[CTA_CONV] = ok;
