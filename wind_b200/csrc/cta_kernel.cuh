@@ -588,6 +588,7 @@ __device__ void cta_solve(const CtaCtx& c, const T* A) {
             }
         }
         double dxm = 0.0, xm = 0.0;
+        bool finite = true;
 #pragma unroll
         for (int m = 0; m < M; m++) {
             const int i = lane + 32 * m;
@@ -596,14 +597,14 @@ __device__ void cta_solve(const CtaCtx& c, const T* A) {
                 c.x[i] = xn;
                 dxm = fmax(dxm, fabs(xr[m]));
                 xm = fmax(xm, fabs(xn));
-                if (!(xr[m] == xr[m])) dxm = xr[m];  // NaN stays visible
+                finite = finite && isfinite(xr[m]) && isfinite(xn);  // (fmax drops NaN)
             }
         }
         if (REFINE) {
-            // converged: on every lane the last correction is below 1e-6 of
-            // the largest |x| among the lane's rows (l, l+32, ...) -- at
-            // least as strict as the same test over all rows
-            int ok = dxm <= 1e-6 * xm;
+            // converged: on every lane the last correction is finite and below
+            // 1e-6 of the largest |x| among the lane's rows (l, l+32, ...) --
+            // at least as strict as the same test over all rows
+            int ok = finite && dxm <= 1e-6 * xm;
             ok = __all_sync(0xffffffffu, ok);
             if (lane == 0) c.misc[CTA_CONV] = ok;
         }
