@@ -75,22 +75,26 @@ wind_status plan_cta(const wind_options& o, const KParams& p, bool allow_global,
     int caps[2] = {smem_optin(), 0};
     int ncap = 1;
     if (solver == WIND_SOLVER_MIXED && CtaMinBlocks<WIND_SOLVER_MIXED>::value >= 2) caps[ncap++] = smem_half(fn);
+    // ranking: the matrix in shared memory first (a matrix in global memory
+    // is read and written on every trailing update), then blocks per SM;
+    // ties keep the larger budget
     bool found = false;
     CtaPlan best{};
-    int best_nb = 0;
+    int best_score = 0;
     for (int i = 0; i < ncap; i++) {
         const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, solver, caps[i]);
         if (lay.bytes > caps[i]) continue;
         if (!allow_global && lay.g_doubles > 0) continue;
         const int nb = cta_blocks_per_sm(fn, lay.bytes);
-        if (nb < 1 || nb <= best_nb) continue;  // ties keep the larger budget
+        const int score = nb + (lay.mat_in_smem ? 1000 : 0);
+        if (nb < 1 || score <= best_score) continue;
         const int64_t resident = (int64_t)nb * device_sm_count();
         best.fn = (const void*)fn;
         best.smem_cap = caps[i];
         best.smem_bytes = lay.bytes;
         best.grid = (int)(p.nsys < resident ? p.nsys : resident);
         best.gstride = lay.g_doubles;
-        best_nb = nb;
+        best_score = score;
         found = true;
     }
     if (!found) return WIND_ERR_UNSUPPORTED;
