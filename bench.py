@@ -1,23 +1,37 @@
 #!/usr/bin/env python
 """Benchmark of the batched stiff-ODE integrators (one JSON line on stdout).
 
-Default workload: the Katz96 primordial H/He network, 65,536 cells with
-T log-U[1e2,1e8] K, nH log-U[1e-4,1e4] cm^-3, UV log-U[1e-15,1e-11] 1/s
-(seed 1), one integration over dt = 1e13 s, FP64 state, SIE, atol 1e-8 /
-rtol 1e-6.  One "step" integrates every cell over the whole interval.
+Default workload -- the metric's own configuration: the synthetic dense stiff
+network, N = 32 species, 262,144 systems (seed 2): J = Q diag(-lambda) Q^T with
+lambda log-U[1e-2,1e6] plus 64 two-body reactions with k log-U[1e-3,1e1],
+y0 U[0,1], integrated over dt = 1 at atol 1e-8 / rtol 1e-6, FP64 state, SIE,
+the c_baseline controller (cuda/c_baseline/common/common_gold.c:48-153, the
+reference arm's own semantics).
 
-* ``value``   systems/s with inputs resident in HBM (CUDA events around each
-              integrate launch; L2 flushed between steps);
-* ``e2e``     the same through the C ABI with pinned host buffers, host<->device
-              copies inside the timed region;
-* ``roofline`` the integrate kernel against the measured FP64 peak (cuBLAS
-              DGEMM timed in this run), algorithmic FLOPs = LU-equivalent count
-              per substep x substeps counted on the device;
-* ``cpu_baseline`` the reference's own CPU integrator (c_baseline, built from
-              the reference sources into oracle/_ref) on a strided sample of the
-              same cells with every host core.
+The whole job -- all 262,144 systems over the full interval -- is timed once:
+the K timed steps are K launches over disjoint contiguous slices that
+together cover every system exactly once.  W warm-up steps run slices before
+the timed region (untimed).
 
-``--impl reference`` times only the reference's CPU integrator on this config.
+* ``value``        systems/s of the MIXED solver (FP32 factors + FP64
+                   refinement) with inputs resident in HBM, CUDA events around
+                   each launch, L2 flushed (256 MB write) between steps;
+* ``solvers``      LU_F64 (plain FP64 LU, slice 0 timed) and GJE_F64 (the
+                   reference's Gauss-Jordan in FP64, rate under a device
+                   deadline) beside it; ``mixed_over_fp64`` = MIXED / LU_F64;
+* ``max_rel_err_vs_reference`` every solver's result on the systems the CPU
+                   baseline integrated, against that run of the reference's
+                   own FP64 c_baseline;
+* ``e2e``          the same metric through the C ABI with pinned host buffers
+                   (host<->device copies inside the timed region);
+* ``roofline``     the integrate kernel against a peak measured in this run;
+* ``cpu_baseline`` the reference's c_baseline (built from its sources into
+                   oracle/_ref) on the first systems, every host core.
+
+``--workload katz96`` (config 2), ``nr`` (config 1), ``ma<N>`` (one class of
+the mixed-size batch), ``mixed`` (the mixed-size batch in one launch) and
+``serve`` (Poisson request streams) select the other workloads.
+``--impl reference`` times only the reference's CPU integrator.
 ``--gpus N`` (under torchrun) runs N independent replicas ("replicas only":
 systems are independent, there is no exchange step).
 """
@@ -44,31 +58,27 @@ METRIC = "systems/s at 1e-5 rel err vs FP64 (mixed vs plain FP64 GPU); serve p50
 
 # ---------------------------------------------------------------------------
 def make_workload(name: str, systems: int = 0, dt: float = 0.0):
+    if name == "dense":
+        n = systems or 262144
+        wl = W.workload_dense(n)
+        t = dt or 1.0
+        wl = W.Workload(wl.net, wl.y0, 0.0, t, wl.atol, wl.rtol, 1, 1, "dense32")
+        return wl, (f"dense N=32 + 64 reactions, {n:,} systems (seed 2), dt={t:g}, "
+                    "atol=1e-8 rtol=1e-6")
     if name == "katz96":
         n = systems or 65536
         wl = W.workload_katz96(n, atol=1e-8, rtol=1e-6)
-        return wl, f"Katz96 5-species, {n:,} cells, dt=1e13 s, atol=1e-8 rtol=1e-6"
-    if name == "katz96_loose":
-        n = systems or 65536
-        wl = W.workload_katz96(n)
-        return wl, f"Katz96 5-species, {n:,} cells, dt=1e13 s, atol=rtol=5e-3"
+        return wl, f"Katz96 5-species, {n:,} cells (seed 1), dt=1e13 s, atol=1e-8 rtol=1e-6"
     if name == "nr":
         wl = W.workload_nr(1024)
         wl = W.Workload(wl.net, wl.y0, 0.0, 0.01, wl.atol, wl.rtol, 1, 1, "nr_test")
         return wl, "NR stiff linear test, 1024 systems, one output interval t=0..0.01"
-    if name == "dense":
-        n = systems or 16384
-        wl = W.workload_dense(n)
-        t = dt or 1.0
-        wl = W.Workload(wl.net, wl.y0, 0.0, t, wl.atol, wl.rtol, 1, 1, "dense32")
-        return wl, f"dense N=32 + 64 reactions, {n:,} systems, dt={t:g}, atol=1e-8 rtol=1e-6"
     if name.startswith("ma"):
-        # one size class of the mixed-size batch: N = int(name[2:]), 10N reactions
         N = int(name[2:])
-        n = systems or 2048
-        t = dt or 1e-3
-        wl = W.workload_mixed(n * 20, seed=3, sizes=(N,), fractions=(1.0,), dt=t)[0].subset(slice(0, n))
-        return wl, (f"mass action N={N}, {10 * N} reactions, {n:,} systems, dt={t:g}, "
+        n = systems or dict(zip(W.MIXED_SIZES, W.mixed_counts(200000)))[N]
+        t = dt or 1.0
+        wl = W.workload_mixed_class(N, n, seed=3, dt=t)
+        return wl, (f"mass action N={N}, {10 * N} reactions, {n:,} systems (seed 3), dt={t:g}, "
                     "atol=1e-8 rtol=1e-6")
     raise SystemExit(f"unknown workload {name}")
 
@@ -91,6 +101,12 @@ def flops_per_substep(wl, method: str) -> float:
     if method == "rk2":
         return f_f + 2.0 * n
     return sie_flops(n, f_f, f_j)
+
+
+def slice_bounds(nsys: int, k: int):
+    """K contiguous slices covering [0, nsys) exactly once."""
+    e = np.linspace(0, nsys, max(1, k) + 1).round().astype(np.int64)
+    return [(int(e[i]), int(e[i + 1])) for i in range(len(e) - 1)]
 
 
 # ---------------------------------------------------------------------------
@@ -149,10 +165,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def measured_fp64_peak(torch, dev):
-    """cuBLAS DGEMM 8192^3, best of 5 (TFLOP/s)."""
-    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
-    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+def measured_gemm_peak(torch, dev, dtype):
+    """cuBLAS GEMM 8192^3 in `dtype` (TF32 off for float32), best of 5 (TFLOP/s)."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, dtype=dtype, device=dev)
+    b = torch.randn(8192, 8192, dtype=dtype, device=dev)
     torch.matmul(a, b)
     torch.cuda.synchronize()
     best = 1e30
@@ -176,54 +193,58 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
-def reference_sample(wl, method: str, target_s: float):
-    """Time the reference c_baseline (oracle/_ref) on a strided sample with
-    every host core.  Returns (systems/s, cores, sample description)."""
+def reference_run(wl, first: int, count: int, method: str, threads: int):
+    """The reference c_baseline (oracle/_ref) on systems [first, first+count):
+    returns (seconds, final state) or (None, reason)."""
     from oracle import pyoracle as O
-    cores = os.cpu_count() or 1
     if not O.reference_available(wl.net, method, "f64"):
-        return None, cores, "oracle/_ref not built"
-    nsys = wl.net.nsys
-    # calibrate on a small strided sample, then size for ~target_s
-    k = max(cores, 64)
-    stride = max(1, nsys // k)
-    sub = wl.subset(slice(0, nsys, stride))
+        return None, "oracle/_ref not built for " + wl.net.name
+    sub = wl.subset(slice(first, first + count))
     y = sub.y0.copy()
     t0 = time.perf_counter()
     O.reference(sub.net, y, sub.tnow, sub.tend, sub.atol, sub.rtol, method,
-                sub.n_integration_steps, threads=cores)
-    dt = time.perf_counter() - t0
-    per = dt / sub.net.nsys
-    want = int(min(nsys, max(sub.net.nsys, target_s / max(per, 1e-9))))
-    stride = max(1, nsys // want)
-    sub = wl.subset(slice(0, nsys, stride))
-    y = sub.y0.copy()
-    t0 = time.perf_counter()
-    O.reference(sub.net, y, sub.tnow, sub.tend, sub.atol, sub.rtol, method,
-                sub.n_integration_steps, threads=cores)
-    dt = time.perf_counter() - t0
-    return sub.net.nsys / dt, cores, f"{sub.net.nsys} of {nsys} cells (every {stride}th), {dt:.1f} s"
+                sub.n_integration_steps, threads=threads)
+    return time.perf_counter() - t0, y
+
+
+def reference_sample_size(wl, method: str, target_s: float, cores: int) -> int:
+    """Systems the reference integrates in about target_s on `cores` threads
+    (calibrated on one system per core)."""
+    n0 = min(wl.net.nsys, cores)
+    dt, _ = reference_run(wl, 0, n0, method, cores)
+    if dt is None:
+        return 0
+    per = dt / max(1, n0) * 1.0  # seconds per system per core-wave
+    waves = max(1.0, target_s / max(dt, 1e-9))
+    return int(min(wl.net.nsys, max(n0, round(waves * n0))))
 
 
 def run_reference_arm(args, wl, desc):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    vals = []
     cores = os.cpu_count() or 1
-    sample = ""
+    per_step = reference_sample_size(wl, args.method, args.ref_seconds, cores)
+    if per_step == 0:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built for " + wl.net.name}))
+        return
+    vals, off, samples = [], 0, []
     for i in range(args.warmup + args.steps):
-        v, cores, sample = reference_sample(wl, args.method, args.ref_seconds)
-        if v is None:
-            print(json.dumps({"impl": "reference", "unavailable": sample}))
-            return
+        if off + per_step > wl.net.nsys:
+            off = 0
+        dt, _ = reference_run(wl, off, per_step, args.method, cores)
         if i >= args.warmup:
-            vals.append(v)
+            vals.append(per_step / dt)
+            samples.append(f"{off}..{off + per_step - 1}")
+        off += per_step
     value = statistics.median(vals)
+    sample = (f"{per_step} systems per step ({args.steps} steps: systems {samples[0]} ... {samples[-1]}), "
+              f"c_baseline FP64 (-Dfloat=double) built from the reference sources, "
+              f"one contiguous shard per thread")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "systems/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": desc, "method": args.method},
+            "data": "synthetic", "config": config_dict(args, wl, desc),
             "cpu_baseline": {"value": value, "unit": "systems/s", "cores": cores,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "systems/s", "h2d_bytes_per_step": 0,
@@ -231,21 +252,300 @@ def run_reference_arm(args, wl, desc):
     print(json.dumps(line), flush=True)
 
 
+def config_dict(args, wl, desc):
+    return {"workload": desc, "method": args.method, "controller": args.controller,
+            "systems": wl.net.nsys, "equations": wl.net.n_eq,
+            "l2": "flushed (256 MB write) between steps",
+            "steps_cover": "the K timed steps are K launches over disjoint slices covering every system once",
+            "parallelism": f"replicas x{int(os.environ.get('WORLD_SIZE', '1'))}"}
+
+
+# ---------------------------------------------------------------------------
+def run_main(args, wl, desc):
+    import ctypes as C
+    import torch
+    from wind_b200 import _capi, lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    wlib = lib.load()
+    stream = torch.cuda.current_stream(dev)
+    net = wl.net
+    N, S = net.n_eq, net.nsys
+    keys = [k for k in ("constants", "rates", "species", "linear") if getattr(net, k) is not None]
+    d_arr = {k: torch.from_numpy(np.ascontiguousarray(getattr(net, k))).to(dev) for k in keys}
+    y0 = torch.from_numpy(wl.y0).to(dev)
+    y = y0.clone()
+    status = torch.zeros(S, dtype=torch.int32, device=dev)
+    nsteps = torch.zeros(S, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+    bounds = slice_bounds(S, args.steps)
+    main_solver = args.solver if args.solver != "auto" else (
+        "mixed" if net.kind == W.NET_MASS_ACTION else "lu_f64")
+
+    def launch(solver, s0, s1, timeout_s=0.0):
+        """One wind_integrate launch over systems [s0, s1) of the resident
+        batch; returns the substeps counted on the device."""
+        o = lib.options(args.method, solver, args.controller, args.spec_width, 0, timeout_s)
+        ns = _capi.network_struct(net, {k: v[s0:s1] for k, v in d_arr.items()})
+        total = C.c_int64(0)
+        code = wlib.wind_integrate(C.byref(o), C.byref(ns), wl.tnow, wl.tend,
+                                   wl.n_integration_steps, y[s0:s1].data_ptr(), s1 - s0, wl.atol,
+                                   wl.rtol, status[s0:s1].data_ptr(), nsteps[s0:s1].data_ptr(),
+                                   C.byref(total), _capi.MEM_DEVICE, stream.cuda_stream)
+        if code != 0:
+            raise RuntimeError(f"wind_integrate failed: {code} {wlib.wind_last_error().decode()}")
+        return int(total.value)
+
+    def timed(solver, s0, s1, timeout_s=0.0):
+        y[s0:s1].copy_(y0[s0:s1])
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        n = launch(solver, s0, s1, timeout_s)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) * 1e-3, n
+
+    # ---- warm-up: W slices of the main solver (untimed)
+    for i in range(args.warmup):
+        timed(main_solver, *bounds[i % len(bounds)])
+
+    # ---- the timed job: every system once, K launches
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = lib.launch_count()
+    times, substeps = [], 0
+    with ClockSampler(local) as clk:
+        for (s0, s1) in bounds:
+            t, n = timed(main_solver, s0, s1)
+            times.append(t)
+            substeps += n
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches = lib.launch_count() - launches0
+    tot = sum(times)
+    if dist is not None:
+        tt = torch.tensor([tot], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot = float(tt.item())
+    value = world * S / tot
+    y_main = y.cpu().numpy()
+    st_main = status.cpu().numpy()
+    steps_main = nsteps.cpu().numpy()
+    results = {main_solver: {"systems_per_s": S / sum(times), "substeps": substeps,
+                             "systems": S, "timed": "all slices",
+                             "flagged_systems": int((st_main != 0).sum())}}
+
+    # ---- the other solvers on slice 0 (LU) / under a deadline (GJE)
+    b0 = bounds[0]
+    outs = {main_solver: y_main}
+    for s in ("lu_f64", "mixed"):
+        if s == main_solver:
+            continue
+        timed(s, b0[0], min(b0[1], b0[0] + 2048))  # warm-up of this kernel
+        t, n = timed(s, *b0)
+        outs[s] = y.cpu().numpy()[b0[0]:b0[1]]
+        results[s] = {"systems_per_s": (b0[1] - b0[0]) / t, "substeps": n, "systems": b0[1] - b0[0],
+                      "timed": "slice 0"}
+    if "gje_f64" not in results:
+        t, n = timed("gje_f64", *b0, timeout_s=args.gje_seconds)
+        per_sys = float(steps_main[b0[0]:b0[1]].mean())
+        results["gje_f64"] = {"substeps_per_s": n / t, "systems_per_s": n / t / per_sys,
+                              "substeps": n, "timed": (f"slice 0 under a {args.gje_seconds:g} s device "
+                                                       "deadline; systems/s = substeps/s / mean "
+                                                       "substeps per system of the main run")}
+    # same-slice ratio (slice 0 of the main run vs LU_F64's slice 0)
+    t_main0 = times[0]
+    if "lu_f64" in results and main_solver != "lu_f64":
+        results["lu_f64"]["main_slice0_s"] = t_main0
+    mixed_over_fp64 = None
+    if "mixed" in results and "lu_f64" in results:
+        if main_solver == "mixed":
+            mixed_over_fp64 = (b0[1] - b0[0]) / t_main0 / results["lu_f64"]["systems_per_s"]
+        else:
+            mixed_over_fp64 = results["mixed"]["systems_per_s"] / (b0[1] - b0[0]) * t_main0
+    mixed_over_gje = None
+    if "mixed" in results:
+        mixed_over_gje = results["mixed"]["systems_per_s"] / results["gje_f64"]["systems_per_s"]
+
+    # ---- e2e through the C ABI with pinned host buffers (first slices)
+    e2e_slices = bounds[:min(len(bounds), args.e2e_slices)]
+    e2e_lo, e2e_hi = e2e_slices[0][0], e2e_slices[-1][1]
+    h_arr = {k: torch.from_numpy(np.ascontiguousarray(getattr(net, k)[e2e_lo:e2e_hi])).pin_memory()
+             for k in keys}
+    h_y0 = torch.from_numpy(np.ascontiguousarray(wl.y0[e2e_lo:e2e_hi])).pin_memory()
+    h_y = torch.empty_like(h_y0).pin_memory()
+    o = lib.options(args.method, main_solver, args.controller, args.spec_width)
+    e2e_times, h2d, d2h = [], 0, 0
+    for (s0, s1) in e2e_slices:
+        a0, a1 = s0 - e2e_lo, s1 - e2e_lo
+        h_y[a0:a1].copy_(h_y0[a0:a1])
+        sub = {k: v[a0:a1] for k, v in h_arr.items()}
+        hns = _capi.network_struct(net, sub)
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        total = C.c_int64(0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        code = wlib.wind_integrate(C.byref(o), C.byref(hns), wl.tnow, wl.tend,
+                                   wl.n_integration_steps, h_y[a0:a1].data_ptr(), s1 - s0, wl.atol,
+                                   wl.rtol, None, None, C.byref(total), _capi.MEM_HOST,
+                                   stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if code != 0:
+            raise RuntimeError(f"e2e wind_integrate failed: {code}")
+        e2e_times.append(e0.elapsed_time(e1) * 1e-3)
+        h2d += (s1 - s0) * N * 8 + sum(v[a0:a1].numel() * v.element_size() for v in h_arr.values())
+        d2h += (s1 - s0) * N * 8 + 8
+    e2e_tot = sum(e2e_times)
+    if dist is not None:
+        tt = torch.tensor([e2e_tot], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_tot = float(tt.item())
+    e2e_sys = e2e_hi - e2e_lo
+    e2e_same = np.array_equal(h_y.numpy(), y_main[e2e_lo:e2e_hi])
+
+    # ---- roofline of the integrate kernel
+    fps = flops_per_substep(wl, args.method)
+    flops = fps * substeps
+    kernel_s = sum(times)
+    achieved = flops / kernel_s / 1e12
+    fp32_main = main_solver == "mixed"
+    peak = measured_gemm_peak(torch, dev, torch.float32 if fp32_main else torch.float64)
+    peak_fp64 = peak if not fp32_main else measured_gemm_peak(torch, dev, torch.float64)
+    alg_bytes = S * (16 * N) + net.nbytes()
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    # DRAM bytes per launch from an ncu capture of the same kernel on a
+    # smaller batch, scaled by systems (every system's network and state cross
+    # HBM once per launch, so traffic grows in proportion to the systems)
+    traffic_per_system = {("dense", "mixed"): args.traffic_per_system,
+                          ("katz96", "lu_f64"): 136.7}.get((args.workload, main_solver), 0.0)
+    traffic = traffic_per_system * S / len(bounds) if traffic_per_system else None
+    roof = {"bound": "fp32" if fp32_main else "fp64", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                               "smaller-batch capture scaled by systems" if traffic else None),
+            "peak_source": ("cuBLAS SGEMM 8192^3 (TF32 off) measured in this run" if fp32_main
+                            else "cuBLAS DGEMM 8192^3 measured in this run"),
+            "frac_of_fp64_peak": achieved / peak_fp64, "fp64_peak": peak_fp64,
+            "flops_per_substep": fps, "substeps": substeps,
+            "hbm": {"alg_bytes_per_launch": alg_bytes / len(bounds),
+                    "achieved_gbs": alg_bytes / kernel_s / 1e9, "peak_gbs": hbm_peak,
+                    "frac": alg_bytes / kernel_s / 1e9 / hbm_peak,
+                    "peak_source": "MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback"}}
+
+    # ---- reference CPU baseline on the first systems, and every solver's
+    # error against its FP64 result on those systems
+    cpu, errs = None, {}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        n_cpu = reference_sample_size(wl, args.method, args.ref_seconds, cores)
+        n_cpu = min(n_cpu, b0[1] - b0[0])
+        if n_cpu > 0:
+            dt, y_ref = reference_run(wl, 0, n_cpu, args.method, cores)
+            cpu = {"value": n_cpu / dt, "unit": "systems/s", "cores": cores, "kind": "reference",
+                   "sample": (f"systems 0..{n_cpu - 1} of {S:,}, {dt:.1f} s; c_baseline FP64 "
+                              "(-Dfloat=double) built from the reference sources")}
+            for s, yy in outs.items():
+                a = yy[:n_cpu]
+                errs[s] = float(np.max(np.abs(a - y_ref) / np.maximum(np.abs(y_ref), wl.atol)))
+            errs["systems"] = n_cpu
+            errs["metric"] = "max |y - y_ref| / max(|y_ref|, atol)"
+
+    # ---- config 2 (Katz96) beside the headline, cheap
+    extra = None
+    if args.workload == "dense" and not args.no_extra:
+        extra = katz96_extra(args, torch, dev, lib, _capi, C)
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(bounds),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 factors + f64 refinement, f64 state" if fp32_main else "f64",
+            "data": "synthetic",
+            "config": dict(config_dict(args, wl, desc), solver=main_solver),
+            "solvers": results, "mixed_over_fp64": mixed_over_fp64,
+            "mixed_over_fp64_definition": "MIXED / LU_F64 systems/s, the same slice 0",
+            "mixed_over_gje_f64": mixed_over_gje,
+            "max_rel_err_vs_reference": errs or None,
+            "e2e": {"value": world * e2e_sys / e2e_tot, "unit": "systems/s",
+                    "h2d_bytes_per_step": int(h2d / len(e2e_slices)),
+                    "d2h_bytes_per_step": int(d2h / len(e2e_slices)),
+                    "systems": e2e_sys, "slices": len(e2e_slices),
+                    "state_equals_resident_run": bool(e2e_same)},
+            "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
+            "clocks": clk.summary(), "config2_katz96": extra}
+    print(json.dumps(line), flush=True)
+
+
+def katz96_extra(args, torch, dev, lib, _capi, C):
+    """Config 2 (Katz96, 65,536 cells, dt = 1e13 s) systems/s per solver."""
+    wl = W.workload_katz96(65536, atol=1e-8, rtol=1e-6)
+    net = wl.net
+    d = {"constants": torch.from_numpy(net.constants).to(dev)}
+    y0 = torch.from_numpy(wl.y0).to(dev)
+    y = y0.clone()
+    stream = torch.cuda.current_stream(dev)
+    wlib = lib.load()
+    out = {}
+    for solver in ("lu_f64", "mixed", "gje_f64"):
+        ts = []
+        for i in range(4):
+            y.copy_(y0)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            o = lib.options("sie", solver, args.controller)
+            ns = _capi.network_struct(net, d)
+            tot = C.c_int64(0)
+            e0.record(stream)
+            code = wlib.wind_integrate(C.byref(o), C.byref(ns), wl.tnow, wl.tend, 1, y.data_ptr(),
+                                       net.nsys, wl.atol, wl.rtol, None, None, C.byref(tot),
+                                       _capi.MEM_DEVICE, stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            if code != 0:
+                raise RuntimeError(f"katz96 {solver}: {code}")
+            if i:
+                ts.append(e0.elapsed_time(e1) * 1e-3)
+        out[solver] = {"systems_per_s": net.nsys / statistics.median(ts), "substeps": int(tot.value)}
+    out["workload"] = "Katz96 5-species, 65,536 cells (seed 1), dt=1e13 s, atol=1e-8 rtol=1e-6"
+    return out
+
+
 # ---------------------------------------------------------------------------
 def run_mixed(args):
     """The mixed-size batch (N in {5,16,32,64,157} at 40/25/20/10/5 %, 10N
     reactions) through wind_integrate_batch -- one persistent launch for all
-    sizes -- timed with CUDA events per solver; one JSON line with systems/s
-    per solver, the MIXED/LU_F64 ratio and MIXED's error vs LU_F64."""
+    sizes -- timed with CUDA events per solver."""
     import torch
     from wind_b200 import lib
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
     nsys = args.systems or 200000
-    dt = args.dt or 1e-4
+    dt = args.dt or 1.0
     groups = W.workload_mixed(nsys, seed=3, dt=dt, atol=1e-8, rtol=1e-6)
     res, ys = {}, {}
-    for solver in ("lu_f64", "mixed"):
+    solvers = ("lu_f64", "mixed") if args.solver == "auto" else (args.solver,)
+    for solver in solvers:
         times = []
         for i in range(args.warmup + args.steps):
             dg = [lib.DeviceGroup(wl, dev) for wl in groups]
@@ -253,7 +553,7 @@ def run_mixed(args):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             stream = torch.cuda.current_stream(dev)
             arr = (lib._capi.WindGroup * len(dg))(*[g.struct() for g in dg])
-            o = lib.options("sie", solver, "device")
+            o = lib.options("sie", solver, args.controller)
             e0.record(stream)
             code = lib.load().wind_integrate_batch(lib.C.byref(o), arr, len(dg), stream.cuda_stream)
             e1.record(stream)
@@ -264,16 +564,20 @@ def run_mixed(args):
                 times.append(e0.elapsed_time(e1) * 1e-3)
         ys[solver] = np.concatenate([g.y.cpu().numpy().ravel() for g in dg])
         res[solver] = {"systems_per_s": nsys / statistics.median(times),
-                       "ms_per_step": 1e3 * statistics.median(times)}
-    a, b = ys["mixed"], ys["lu_f64"]
-    err = float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-8)))
+                       "ms_per_step": 1e3 * statistics.median(times),
+                       "substeps": int(sum(int(g.nsteps.sum()) for g in dg)),
+                       "flagged_systems": int(sum(int((g.status != 0).sum()) for g in dg))}
     line = {"metric": METRIC, "workload": "mixed", "unit": "systems/s",
-            "value": res["mixed"]["systems_per_s"], "steps": args.steps, "warmup": args.warmup,
+            "value": res[solvers[-1]]["systems_per_s"], "steps": args.steps, "warmup": args.warmup,
             "config": {"workload": (f"{nsys:,} systems, N in {{5,16,32,64,157}} at 40/25/20/10/5 %, "
-                                    f"10N reactions, dt={dt:g}, atol 1e-8 rtol 1e-6, one persistent "
-                                    "launch (wind_integrate_batch)")},
-            "solvers": res, "mixed_over_fp64": res["mixed"]["systems_per_s"] / res["lu_f64"]["systems_per_s"],
-            "max_rel_err_mixed_vs_fp64": err}
+                                    f"10N reactions (seed 3), dt={dt:g}, atol 1e-8 rtol 1e-6, one "
+                                    "persistent launch (wind_integrate_batch)"),
+                       "controller": args.controller},
+            "solvers": res}
+    if len(solvers) == 2:
+        a, b = ys["mixed"], ys["lu_f64"]
+        line["mixed_over_fp64"] = res["mixed"]["systems_per_s"] / res["lu_f64"]["systems_per_s"]
+        line["max_rel_err_mixed_vs_lu_f64"] = float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-8)))
     print(json.dumps(line), flush=True)
 
 
@@ -288,7 +592,7 @@ def run_serve(args):
     for i, rate in enumerate(rates):
         reqs = serve.request_stream(args.requests, seed=4 + i, max_cells=args.max_cells,
                                     dt_range=(args.dt_lo, args.dt_hi), atol=1e-6, rtol=1e-4)
-        with serve.Server(solver=args.solver if args.solver != "auto" else "lu_f64",
+        with serve.Server(solver=args.solver if args.solver != "auto" else "mixed",
                           max_inflight=4) as srv:
             serve.poisson_load(srv, reqs[:8], rate)  # warm-up
             summary, _ = serve.poisson_load(srv, reqs, rate)
@@ -310,15 +614,26 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="wind", choices=["wind", "reference"])
-    ap.add_argument("--workload", default="katz96")
+    ap.add_argument("--workload", default="dense")
     ap.add_argument("--systems", type=int, default=0, help="override the system count "
                     "(profiling runs on a small case; the headline uses the default)")
     ap.add_argument("--dt", type=float, default=0.0, help="interval override (profiling cases)")
     ap.add_argument("--method", default="sie", choices=["sie", "rk2"])
     ap.add_argument("--solver", default="auto", choices=["auto", "gje_f64", "lu_f64", "mixed"])
+    ap.add_argument("--controller", default="gold", choices=["gold", "device"])
     ap.add_argument("--spec-width", type=int, default=0)
-    ap.add_argument("--ref-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--gje-seconds", type=float, default=3.0)
+    ap.add_argument("--e2e-slices", type=int, default=3)
+    ap.add_argument("--traffic-per-system", type=float, default=0.0,
+                    help="DRAM bytes per system per launch from an ncu capture (roofline.traffic)")
+    ap.add_argument("--profile", action="store_true",
+                    help="launch only the chosen solver's integrate kernel (warm-up + steps launches "
+                         "on the first --systems systems) -- the small case an ncu capture runs")
+    ap.add_argument("--deadline", type=float, default=0.0,
+                    help="device deadline per launch in seconds (bounds a profiled launch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--rates", default="10,30,100,300,1000,2000", help="serving request rates (Hz)")
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--max-cells", type=int, default=2000)
@@ -334,192 +649,38 @@ def main():
     wl, desc = make_workload(args.workload, args.systems, args.dt)
     if args.impl == "reference":
         return run_reference_arm(args, wl, desc)
+    if args.profile:
+        return run_profile(args, wl, desc)
+    return run_main(args, wl, desc)
 
+
+def run_profile(args, wl, desc):
+    """Warm-up + K launches of one solver on the resident batch, nothing
+    else on the GPU: the command an ncu capture of the integrate kernel runs."""
     import torch
-    import ctypes as C
-    from wind_b200 import lib, _capi
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    wlib = lib.load()
-    stream = torch.cuda.current_stream(dev)
-    net = wl.net
-    N = net.n_eq
-    d_arrays = {}
-    for k in ("constants", "rates", "species", "linear"):
-        a = getattr(net, k)
-        if a is not None:
-            d_arrays[k] = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
-    ns = _capi.network_struct(net, d_arrays)
+    from wind_b200 import lib
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    solver = args.solver if args.solver != "auto" else (
+        "mixed" if wl.net.kind == W.NET_MASS_ACTION else "lu_f64")
+    d_arr = {k: torch.from_numpy(np.ascontiguousarray(getattr(wl.net, k))).to(dev)
+             for k in ("constants", "rates", "species", "linear") if getattr(wl.net, k) is not None}
     y0 = torch.from_numpy(wl.y0).to(dev)
-    y = torch.empty_like(y0)
-    status = torch.zeros(net.nsys, dtype=torch.int32, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
-
-    def run_once(solver, width, ybuf):
-        o = lib.options(args.method, solver, "device", width)
-        total = C.c_int64(0)
-        code = wlib.wind_integrate(C.byref(o), C.byref(ns), wl.tnow, wl.tend,
-                                   wl.n_integration_steps, ybuf.data_ptr(), net.nsys, wl.atol,
-                                   wl.rtol, status.data_ptr(), None, C.byref(total),
-                                   _capi.MEM_DEVICE, stream.cuda_stream)
-        if code != 0:
-            raise RuntimeError(f"wind_integrate failed: {code}")
-        return int(total.value)
-
-    def timed(solver, width, steps, warmup):
-        times, substeps = [], 0
-        for i in range(warmup + steps):
-            y.copy_(y0)
-            flush.zero_()
-            if dist is not None:
-                dist.barrier()
-            torch.cuda.synchronize(dev)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            n = run_once(solver, width, y)
-            e1.record(stream)
-            torch.cuda.synchronize(dev)
-            if i >= warmup:
-                times.append(e0.elapsed_time(e1) * 1e-3)
-                substeps = n
-        return times, substeps
-
-    # FP64 reference result on the device (the reference algorithm, GJE_F64)
-    run_once("gje_f64", args.spec_width, y.copy_(y0))
-    torch.cuda.synchronize(dev)
-    y_ref = y.clone()
-
-    solvers = ["gje_f64", "lu_f64", "mixed"] if args.solver == "auto" else [args.solver]
-    results = {}
-    for s in solvers:
-        t, nsub = timed(s, args.spec_width, max(2, args.steps // 3), 1)
-        run_once(s, args.spec_width, y.copy_(y0))
-        torch.cuda.synchronize(dev)
-        a, b = y.cpu().numpy(), y_ref.cpu().numpy()
-        err = float(np.max(np.abs(a - b) / np.maximum(np.abs(b), wl.atol)))
-        results[s] = {"systems_per_s": net.nsys / statistics.median(t), "substeps": nsub,
-                      "max_rel_err_vs_fp64": err}
-    ok = [s for s in solvers if results[s]["max_rel_err_vs_fp64"] <= 1e-5]
-    best = max(ok, key=lambda s: results[s]["systems_per_s"]) if ok else "gje_f64"
-    width = args.spec_width
-    tuning = None
-    if args.solver == "auto" and args.spec_width == 0 and net.kind != W.NET_MASS_ACTION:
-        # initial lanes per system (autotuner): widths 1..8 for the chosen solver
-        from wind_b200 import autotune
-        tbest, table = autotune.tune(wl, args.method, "device", widths=(1, 2, 4, 8),
-                                     solvers=(best,))
-        tuning = table
-        if tbest["solver"] == best:
-            width = tbest["spec_width"]
-
-    # the timed run of the chosen path
-    launches0 = lib.launch_count()
-    with ClockSampler(local) as clk:
-        times, nsub = timed(best, width, args.steps, args.warmup)
-    launches = lib.launch_count() - launches0
-    launches = launches * args.steps // (args.steps + args.warmup)
-    tot = sum(times)
-    if dist is not None:
-        tt = torch.tensor([tot], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        tot = float(tt.item())
-    value = world * net.nsys * args.steps / tot
-    ms_per_step = 1e3 * tot / args.steps
-
-    # e2e through the C ABI with pinned host buffers
-    h_y0 = torch.from_numpy(wl.y0).pin_memory()
-    h_y = torch.empty_like(h_y0).pin_memory()
-    h_arr = {k: torch.from_numpy(np.ascontiguousarray(getattr(net, k))).pin_memory()
-             for k in ("constants", "rates", "species", "linear") if getattr(net, k) is not None}
-    hns = _capi.network_struct(net, h_arr)
-    o = lib.options(args.method, best, "device", width)
-    e2e_times = []
+    out = []
     for i in range(args.warmup + args.steps):
-        h_y.copy_(h_y0)
-        flush.zero_()
+        y = y0.clone()
         torch.cuda.synchronize(dev)
-        total = C.c_int64(0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        code = wlib.wind_integrate(C.byref(o), C.byref(hns), wl.tnow, wl.tend,
-                                   wl.n_integration_steps, h_y.data_ptr(), net.nsys, wl.atol,
-                                   wl.rtol, None, None, C.byref(total), _capi.MEM_HOST,
-                                   stream.cuda_stream)
-        e1.record(stream)
+        e0.record()
+        tot, st, _ = lib.integrate(wl.net, y, wl.tnow, wl.tend, wl.atol, wl.rtol, args.method, solver,
+                                   args.controller, timeout_s=args.deadline, device_arrays=d_arr)
+        e1.record()
         torch.cuda.synchronize(dev)
-        if code != 0:
-            raise RuntimeError(f"e2e wind_integrate failed: {code}")
         if i >= args.warmup:
-            e2e_times.append(e0.elapsed_time(e1) * 1e-3)
-    e2e_tot = sum(e2e_times)
-    if dist is not None:
-        tt = torch.tensor([e2e_tot], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_tot = float(tt.item())
-    h2d = int(wl.y0.nbytes + sum(v.numel() * v.element_size() for v in h_arr.values()))
-    d2h = int(wl.y0.nbytes + 8)
-
-    # roofline of the integrate kernel (FP64 pipe)
-    flops = flops_per_substep(wl, args.method) * nsub
-    kernel_s = statistics.median(times)
-    achieved = flops / kernel_s / 1e12
-    peak = measured_fp64_peak(torch, dev)
-    alg_bytes = net.nsys * (16 * N) + net.nbytes()
-    peaks = measured_peaks()
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    # DRAM bytes per launch from the committed ncu capture of the Katz96
-    # kernel (profiles/k_lane_katz96_lu_16384cells.md: 2.000 MB read + 0.239
-    # MB written for 16,384 cells, i.e. 136.7 B per cell; every cell's state
-    # and constants cross HBM once, so it scales with the cell count)
-    traffic = 136.7 * net.nsys if net.kind == W.NET_KATZ96 else None
-    roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": traffic,
-            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, 16,384-cell "
-                               "capture scaled by cells" if traffic is not None else None),
-            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-            "flops_per_substep": flops_per_substep(wl, args.method), "substeps_per_launch": nsub,
-            "hbm": {"alg_bytes_per_launch": alg_bytes,
-                    "achieved_gbs": alg_bytes / kernel_s / 1e9, "peak_gbs": hbm_peak,
-                    "frac": alg_bytes / kernel_s / 1e9 / hbm_peak,
-                    "peak_source": "MEASURED_PEAKS.json" if "hbm_gbs" in peaks else "fallback"}}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, sample = reference_sample(wl, args.method, args.ref_seconds)
-        if v is not None:
-            cpu = {"value": v, "unit": "systems/s", "cores": cores, "kind": "reference",
-                   "sample": sample + "; c_baseline FP64 (-Dfloat=double) built from the reference sources"}
-
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    line = {"metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": desc, "method": args.method, "solver": best,
-                       "controller": "device (cuda/common/kernel.cu semantics)",
-                       "systems": net.nsys, "equations": N, "l2": "flushed (256 MB write) between steps",
-                       "parallelism": f"replicas x{world}"},
-            "solvers": results, "spec_width": width, "tuning": tuning,
-            "max_rel_err_vs_fp64": results[best]["max_rel_err_vs_fp64"],
-            "e2e": {"value": world * net.nsys * args.steps / e2e_tot, "unit": "systems/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-            "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+            out.append({"ms": e0.elapsed_time(e1), "substeps": tot,
+                        "flagged": int((st.cpu().numpy() != 0).sum())})
+    print(json.dumps({"profile": desc, "solver": solver, "controller": args.controller,
+                      "deadline_s": args.deadline, "launches": out}), flush=True)
 
 
 if __name__ == "__main__":

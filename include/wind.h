@@ -176,7 +176,12 @@ int wind_integrate_batch(const wind_options* opt, const wind_group* groups,
  * clears what it uses first, so calls in sequence are independent, while
  * calls that overlap on the GPU race and must not be issued.  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress);
- * make it before any stream capture on that device. */
+ * make it before any stream capture on that device (the lookup is repeated
+ * only if the device's CUDA context changed, e.g. after a device reset).  A
+ * group whose kernels would need matrix scratch in global memory (mass
+ * action with N > 32 whose factor does not fit in shared memory, or
+ * Gauss-Jordan with N > 32) makes the whole call return WIND_ERR_UNSUPPORTED
+ * before any group is cleared or launched: no state is changed. */
 #define WIND_NOALLOC_MAX_GROUPS 256
 int wind_integrate_batch_noalloc(const wind_options* opt, const wind_group* groups,
                                  int32_t ngroups, void* stream);

@@ -45,7 +45,7 @@ def layouts(tmp_path_factory):
     src = d / "probe.cu"
     src.write_text(PROBE)
     exe = d / "probe"
-    subprocess.run([nvcc, "-std=c++17", "--expt-relaxed-constexpr", "-I",
+    subprocess.run([nvcc, "-std=c++17", "--expt-relaxed-constexpr", "-gencode", "arch=compute_100a,code=sm_100a", "-I",
                     os.path.join(ROOT, "wind_b200", "csrc"), "-o", str(exe), str(src)],
                    check=True, capture_output=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout

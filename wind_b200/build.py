@@ -28,7 +28,7 @@ FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 
 # translation units of libwind.so
 UNITS = ["api", "batch", "noalloc", "dispatch_lane", "dispatch_team", "dispatch_team8",
-         "dispatch_team16", "dispatch_team32", "dispatch_cta", "dispatch_mixed", "server"]
+         "dispatch_team16", "dispatch_team32", "dispatch_warp", "dispatch_cta", "dispatch_mixed", "server"]
 
 LEGACY_NETS = {"nr_test": "WIND_NET_NR_TEST", "katz96": "WIND_NET_KATZ96",
                "stifftrig": "WIND_NET_STIFFTRIG"}
@@ -38,6 +38,20 @@ LEGACY_METHODS = {"sie": "WIND_METHOD_SIE", "rk2": "WIND_METHOD_RK2"}
 def _deps():
     return (glob.glob(os.path.join(CSRC, "*")) +
             [os.path.join(ROOT, "include", "wind.h"), os.path.join(ROOT, "include", "wind_legacy.h")])
+
+
+def _unit_deps(path, seen=None):
+    """The file and every local header it includes, recursively."""
+    import re
+    seen = set() if seen is None else seen
+    path = os.path.normpath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as fh:
+        for inc in re.findall(r'^\s*#include\s+"([^"]+)"', fh.read(), re.M):
+            _unit_deps(os.path.join(os.path.dirname(path), inc), seen)
+    return seen
 
 
 def _stale(target, deps):
@@ -66,7 +80,7 @@ def build_native(verbose=False):
     for unit in UNITS:
         obj = os.path.join(OBJ, unit + ".o")
         objs.append(obj)
-        if _stale(obj, deps):
+        if _stale(obj, sorted(_unit_deps(os.path.join(CSRC, unit + ".cu")))):
             if verbose:
                 print(f"nvcc {unit}.cu", flush=True)
             jobs.append(([NVCC] + FLAGS + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj],

@@ -134,9 +134,7 @@ int wind_integrate(const wind_options* opt_in, const wind_network* net, double t
     wind_options o;
     if (opt_in) o = *opt_in; else wind_default_options(&o);
     (void)cudaGetLastError();  // an earlier, unrelated error is not this call's
-    if (o.method != WIND_METHOD_SIE && o.method != WIND_METHOD_RK2) return WIND_ERR_ARGUMENT;
-    if (o.controller != WIND_CTRL_DEVICE && o.controller != WIND_CTRL_GOLD) return WIND_ERR_ARGUMENT;
-    if (o.solver < WIND_SOLVER_GJE_F64 || o.solver > WIND_SOLVER_MIXED) return WIND_ERR_ARGUMENT;
+    if (check_options(o) != WIND_OK) return WIND_ERR_ARGUMENT;
     if (nsys < 0 || n_integration_steps < 1) return WIND_ERR_ARGUMENT;
     if (memory != WIND_MEM_HOST && memory != WIND_MEM_DEVICE) return WIND_ERR_ARGUMENT;
     wind_status st = check_network(net, nsys);
@@ -169,6 +167,7 @@ int wind_integrate_output_steps(const wind_options* opt_in, const wind_network* 
     if (opt_in) o = *opt_in; else wind_default_options(&o);
     if (n_output_steps < 1 || n_integration_steps < 1 || nsys < 0) return WIND_ERR_ARGUMENT;
     (void)cudaGetLastError();
+    if (check_options(o) != WIND_OK) return WIND_ERR_ARGUMENT;
     if (memory != WIND_MEM_HOST && memory != WIND_MEM_DEVICE) return WIND_ERR_ARGUMENT;
     wind_status st = check_network(net, nsys);
     if (st != WIND_OK) return st;
@@ -272,5 +271,6 @@ extern "C" int wind_integrate_batch(const wind_options* opt_in, const wind_group
     if (opt_in) o = *opt_in; else wind_default_options(&o);
     if (ngroups < 0 || (ngroups > 0 && !groups)) return WIND_ERR_ARGUMENT;
     (void)cudaGetLastError();
+    if (wind::check_options(o) != WIND_OK) return WIND_ERR_ARGUMENT;
     return wind::launch_batch(o, groups, ngroups, (cudaStream_t)stream_v);
 }

@@ -12,6 +12,16 @@ namespace wind {
 
 int device_sm_count();
 wind_status check_network(const wind_network* net, int64_t nsys);
+
+// Range checks of the options every entry point applies: an unknown method,
+// controller or solver is an argument error, never read as a default.
+inline wind_status check_options(const wind_options& o) {
+    if (o.method != WIND_METHOD_SIE && o.method != WIND_METHOD_RK2) return WIND_ERR_ARGUMENT;
+    if (o.controller != WIND_CTRL_DEVICE && o.controller != WIND_CTRL_GOLD) return WIND_ERR_ARGUMENT;
+    if (o.solver < WIND_SOLVER_GJE_F64 || o.solver > WIND_SOLVER_MIXED) return WIND_ERR_ARGUMENT;
+    if (o.spec_width < 0 || o.max_attempts < 0 || !(o.timeout_s >= 0.0)) return WIND_ERR_ARGUMENT;
+    return WIND_OK;
+}
 // Launch the kernel family for one homogeneous batch.  `allow_alloc` = false
 // makes configurations that need global scratch return WIND_ERR_UNSUPPORTED
 // instead of taking it from the stream-ordered allocator.

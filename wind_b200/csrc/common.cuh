@@ -88,6 +88,11 @@ __device__ __forceinline__ float nr_rcp(float b) {
     return fmaf(y, e, y);
 }
 
+// |a| as a float bit pattern: monotone for non-negative values, and a NaN
+// sorts above +inf, so a max-reduction over these keys never reads a NaN
+// correction as small.
+__device__ __forceinline__ unsigned fmax_bits(double a) { return __float_as_uint((float)fabs(a)); }
+
 // Refinement cap before an attempt is accepted regardless of its error:
 // kernel.cu:259 (RK2 20, SIE 10) for DEVICE, common_gold.c:121 (10) for GOLD.
 template <int METHOD, int CTRL>

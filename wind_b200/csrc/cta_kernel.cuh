@@ -244,7 +244,7 @@ __device__ __forceinline__ void cta_incidences(const CtaCtx& c, int j, F&& fn) {
 // not bit-exact by design; the reference-order evaluation is cta_rhs /
 // cta_gje_exact.)
 template <typename T>
-__device__ void cta_build(const CtaCtx& c, double h, T* A) {
+__device__ __noinline__ void cta_build(const CtaCtx& c, double h, T* A) {
     const int N = c.N, j = c.tid, ld = c.ld;
     const int q4 = c.cols >> 2;  // 4-wide chunks per row that hold data
     if (j < N) {
@@ -276,6 +276,22 @@ __device__ void cta_build(const CtaCtx& c, double h, T* A) {
             }
             st4(row + 4 * q, a);
         }
+    }
+    __syncthreads();
+}
+
+// f_j for j = tid at the state in c.v, FP64 with fused multiply-adds (the
+// mixed solver's right-hand side; the bit-exact evaluation is cta_rhs).
+__device__ __forceinline__ void cta_rhs_fast(const CtaCtx& c) {
+    const int N = c.N, j = c.tid;
+    if (j < N) {
+        double acc = 0.0;
+        if (c.LT)
+            for (int k = 0; k < N; k++) acc = fma((double)c.LT[k * N + j], c.v[k], acc);
+        cta_incidences<4>(c, j, [&](double k, int a, int b, double sg) {
+            acc = fma(sg * k * c.v[a], c.v[b], acc);
+        });
+        c.f[j] = acc;
     }
     __syncthreads();
 }
@@ -612,6 +628,233 @@ __device__ void cta_solve(const CtaCtx& c, const T* A) {
     __syncthreads();
 }
 
+// ---- MIXED: FP32 Gauss-Jordan inverse reused across an attempt ----------
+// misc[] slots 8..10: rotating CTA-wide maxima (unsigned float bits).
+constexpr int CTA_MAXSLOT = 8;
+
+// CTA-wide max of |v| (one barrier).  `phase` rotates over three slots; the
+// slot of the next call is cleared here -- its last readers read it two
+// calls ago, before the barrier of the previous call.
+__device__ __forceinline__ double cta_max_abs(const CtaCtx& c, double v, int& phase) {
+    unsigned* slot = reinterpret_cast<unsigned*>(c.misc + CTA_MAXSLOT);
+    const unsigned w = __reduce_max_sync(0xffffffffu, fmax_bits(v));
+    if ((c.tid & 31) == 0) atomicMax(slot + phase, w);
+    if (c.tid == 0) slot[(phase + 1) % 3] = 0u;
+    __syncthreads();
+    const unsigned m = slot[phase];
+    phase = (phase + 1) % 3;
+    return (double)__uint_as_float(m);
+}
+
+// Unpivoted blocked Gauss-Jordan inversion of A (N x N, FP32, row stride
+// c.ld, shared memory) in place.  Per panel P = [k0, k0+kb) with the other
+// indices R = [0, N) \ P:
+//  1. warp 0 inverts D = A[P][P] in registers (element Gauss-Jordan with
+//     shuffles; lane i holds row i of D);
+//  2. A[P][R] <- D^-1 A[P][R]          one thread per column of R;
+//  3. A[R][R] <- A[R][R] - A[R][P] A[P][R]   4x4 register tiles over the
+//     4-aligned row and column chunks that miss P (the rank-kb update);
+//  4. A[R][P] <- -A[R][P] D^-1         one thread per row of R.
+// Four CTA barriers per panel.  Without pivoting the diagonal blocks must be
+// invertible; a bad inverse shows up as a refinement that does not converge.
+static __device__ __noinline__ void cta_gj_invert(const CtaCtx& c, float* A) {
+    const int N = c.N, tid = c.tid, ld = c.ld;
+    const int nch = (N + 3) >> 2;  // 4-wide chunks holding rows / columns < N
+    for (int k0 = 0; k0 < N; k0 += CTA_NB) {
+        const int kb = min(CTA_NB, N - k0);
+        const int pc0 = k0 >> 2, pc1 = (k0 + kb + 3) >> 2;  // chunks touching P
+        // 1. D^-1 on warp 0
+        if (tid < 32) {
+            const int lane = tid;
+            const bool mine = lane < kb;
+            float d[CTA_NB];
+            const float* row = A + (size_t)(k0 + (mine ? lane : 0)) * ld + k0;
+#pragma unroll
+            for (int q = 0; q < CTA_NB / 4; q++) ld4at(row + 4 * q, d + 4 * q);
+#pragma unroll
+            for (int q = 0; q < CTA_NB; q++)
+                if (!mine || q >= kb) d[q] = 0.0f;
+#pragma unroll
+            for (int k = 0; k < CTA_NB; k++) {
+                if (k < kb) {
+                    const float r = nr_rcp(__shfl_sync(0xffffffffu, d[k], k));
+                    const float f = (lane == k) ? 0.0f : d[k] * r;
+#pragma unroll
+                    for (int q = 0; q < CTA_NB; q++) {
+                        const float pq = __shfl_sync(0xffffffffu, d[q], k);
+                        if (q != k) d[q] = (lane == k) ? d[q] * r : fmaf(-f, pq, d[q]);
+                    }
+                    d[k] = (lane == k) ? r : -f;
+                }
+            }
+            if (mine) {
+                float* wrow = A + (size_t)(k0 + lane) * ld + k0;
+#pragma unroll
+                for (int q = 0; q < CTA_NB; q++)
+                    if (q < kb) wrow[q] = d[q];
+            }
+        }
+        __syncthreads();
+        // 2. row panel: one thread per column of R
+        for (int t = tid; t < N - kb; t += CTA_THREADS) {
+            const int j = t < k0 ? t : t + kb;
+            float u[CTA_NB];
+#pragma unroll
+            for (int q = 0; q < CTA_NB; q++) u[q] = q < kb ? A[(size_t)(k0 + q) * ld + j] : 0.0f;
+            // the column is in registers: each result is stored as it is formed
+#pragma unroll
+            for (int q = 0; q < CTA_NB; q++) {
+                if (q < kb) {
+                    const float* drow = A + (size_t)(k0 + q) * ld + k0;
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int pp = 0; pp < CTA_NB; pp++)
+                        if (pp < kb) acc = fmaf(drow[pp], u[pp], acc);
+                    A[(size_t)(k0 + q) * ld + j] = acc;
+                }
+            }
+        }
+        __syncthreads();
+        // 3. rank-kb update of R x R over 4x4 tiles of the chunks missing P
+        {
+            const int m4 = nch - (pc1 - pc0);  // chunks outside P
+            for (int t = tid; t < m4 * m4; t += CTA_THREADS) {
+                const int ti = t / m4, tj = t - ti * m4;
+                const int ri = ti < pc0 ? ti : ti + (pc1 - pc0);
+                const int cj = tj < pc0 ? tj : tj + (pc1 - pc0);
+                const int col = 4 * cj;
+                float acc[4][4];
+                int rows[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    const int i = 4 * ri + r;
+                    rows[r] = i < N ? i * ld : -1;
+                    if (rows[r] >= 0) ld4(A + rows[r] + col, acc[r]);
+                    else acc[r][0] = acc[r][1] = acc[r][2] = acc[r][3] = 0.0f;
+                }
+#pragma unroll 1
+                for (int q0 = 0; q0 < CTA_NB; q0 += 4) {
+                    float u[4][4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (q0 + q < kb) ld4(A + (size_t)(k0 + q0 + q) * ld + col, u[q]);
+                        else u[q][0] = u[q][1] = u[q][2] = u[q][3] = 0.0f;
+                    }
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        float l[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                        if (rows[r] >= 0) ld4(A + rows[r] + k0 + q0, l);
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            const float lq = (q0 + q < kb) ? l[q] : 0.0f;
+#pragma unroll
+                            for (int cc = 0; cc < 4; cc++) acc[r][cc] = fmaf(-lq, u[q][cc], acc[r][cc]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+                    if (rows[r] >= 0) st4(A + rows[r] + col, acc[r]);
+            }
+        }
+        __syncthreads();
+        // 4. column panel: one thread per row of R
+        for (int t = tid; t < N - kb; t += CTA_THREADS) {
+            const int i = t < k0 ? t : t + kb;
+            float* row = A + (size_t)i * ld + k0;
+            float l[CTA_NB];
+#pragma unroll
+            for (int q = 0; q < CTA_NB; q++) l[q] = q < kb ? row[q] : 0.0f;
+            // the row segment is in registers: each result is stored as it is formed
+#pragma unroll
+            for (int pp = 0; pp < CTA_NB; pp++) {
+                if (pp < kb) {
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < CTA_NB; q++)
+                        if (q < kb) acc = fmaf(l[q], A[(size_t)(k0 + q) * ld + k0 + pp], acc);
+                    row[pp] = -acc;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Row j of M times the FP32 vector qb (shared memory), four accumulators.
+__device__ __forceinline__ double cta_apply_row(const float* mrow, const float* qb, int N) {
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    const int n4 = N & ~3;
+    for (int k = 0; k < n4; k += 4) {
+        float a[4];
+        ld4(mrow + k, a);
+        const float4 b = *reinterpret_cast<const float4*>(qb + k);
+        s0 = fmaf(a[0], b.x, s0);
+        s1 = fmaf(a[1], b.y, s1);
+        s2 = fmaf(a[2], b.z, s2);
+        s3 = fmaf(a[3], b.w, s3);
+    }
+    for (int k = n4; k < N; k++) s0 = fmaf(mrow[k], qb[k], s0);
+    return (double)((s0 + s1) + (s2 + s3));
+}
+
+enum { CTA_REFINE_OK = 0, CTA_REFINE_GAVE_UP = 1 };
+
+// FP64 iterative refinement of (I - h J(v)) x = f (v in c.v, f in c.f)
+// around the approximate inverse A: x = M f, then r = f - (x - h J x),
+// x += M r.  Stop and give-up rules as the team kernel's (predicted error
+// below 2^-33 max|x|; contraction worse than `abort0` on the first sweep or
+// 1/2 later).  The result is left in c.x (natural order).  Uniform across
+// the CTA.
+static __device__ __noinline__ int cta_refine(const CtaCtx& c, const float* A, double h, int maxit, double abort0,
+                          int& phase) {
+    const int N = c.N, j = c.tid, ld = c.ld;
+    const bool own = j < N;
+    // FP32 broadcast vector in the residual slot (c.r starts 32N bytes into
+    // the 16-byte aligned vector block, so float4 reads of it are aligned)
+    float* qb = reinterpret_cast<float*>(c.r);
+    if (own) qb[j] = (float)c.f[j];
+    __syncthreads();
+    double xj = own ? cta_apply_row(A + (size_t)j * ld, qb, N) : 0.0;
+    const double xmax = cta_max_abs(c, xj, phase);
+    double dprev = 0.0;
+    int outcome = CTA_REFINE_GAVE_UP;
+    for (int it = 0; it < maxit; it++) {
+        if (own) c.x[j] = xj;
+        __syncthreads();
+        const double r = own ? c.f[j] - fma(-h, cta_jx(c, j, c.x), xj) : 0.0;
+        if (own) qb[j] = (float)r;
+        __syncthreads();
+        const double d = own ? cta_apply_row(A + (size_t)j * ld, qb, N) : 0.0;
+        xj += d;
+        const double dmax = cta_max_abs(c, d, phase);
+        const double rho = (it == 0) ? dmax / fmax(xmax, 1e-300) : dmax / fmax(dprev, 1e-300);
+        if (dmax * rho <= 0x1p-33 * xmax || dmax == 0.0) { outcome = CTA_REFINE_OK; break; }
+        if (rho > (it == 0 ? abort0 : 0.5)) break;
+        dprev = dmax;
+    }
+    if (own) c.x[j] = xj;
+    __syncthreads();
+    return outcome;
+}
+
+// The substep solve with pivoting (FP32 LU with partial pivoting and up to
+// two FP64 refinement sweeps): the recovery path when the Gauss-Jordan
+// inverse does not refine.  Builds [I - hJ(v) | f] itself; result in c.x.
+static __device__ __noinline__ void cta_mixed_pivoted_solve(const CtaCtx& c, double h, float* A) {
+    const int tid = c.tid;
+    const bool own = tid < c.N;
+    cta_build<float>(c, h, A);
+    cta_lu<float>(c, A);
+    cta_solve<float, false>(c, A);
+    for (int it = 0; it < 2; it++) {
+        if (own) c.r[tid] = c.f[tid] - (c.x[tid] - h * cta_jx(c, tid, c.x));
+        __syncthreads();
+        cta_solve<float, true>(c, A);
+        if (c.misc[CTA_CONV]) break;
+    }
+}
+
 // The reference Gauss-Jordan inverse, CTA-parallel, on global scratch.
 // M = I - hJt in the reference orientation (rows of Jt), Inv starts as I.
 template <int CTRL>
@@ -856,6 +1099,7 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
             }
         }
         double yl = own ? p.y[s * N + tid] : 0.0, y1l = 0.0, y2l = 0.0;
+        if (tid < 3) reinterpret_cast<unsigned*>(c.misc + CTA_MAXSLOT)[tid] = 0u;
         __syncthreads();
 
         double tnow = p.tnow;
@@ -864,6 +1108,11 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
         int unsolved = 0;
         int64_t attempts = 0;
         int32_t st = bad ? WIND_SYS_BAD_INPUT : WIND_SYS_OK;
+        // MIXED: f(y) cached while y is unchanged; the matrix area holds the
+        // inverse for the next full step; rotating max-slot phase
+        bool fy_ok = false, inv_ok = false;
+        double fyl = 0.0;
+        int phase = 0;
         while (!bad && tnow < tend) {
             if (attempts >= p.max_attempts) { st |= WIND_SYS_MAX_ATTEMPTS; break; }
             if (p.timeout_ns) {
@@ -876,6 +1125,58 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
             attempts++;
             h = fmin(tend - tnow, h);
             const double t1 = tnow + h;
+            if constexpr (METHOD == WIND_METHOD_SIE && SOLVER == WIND_SOLVER_MIXED) {
+                // One FP32 Gauss-Jordan inverse serves the attempt: the
+                // previous attempt's half-step inverse (same y, same size)
+                // for the full step, a fresh one for the first half step,
+                // reused for the second half step while it still contracts.
+                const double hf = t1 - tnow, h1 = (t1 - tnow) * 0.5;
+                const double h2 = (CTRL == WIND_CTRL_DEVICE) ? fmin(t1 - (tnow + h1), h1) : h1;
+                float* A = static_cast<float*>(mat);
+                if (own) c.v[tid] = yl;
+                __syncthreads();
+                if (!fy_ok) {
+                    cta_rhs_fast(c);
+                    fyl = own ? c.f[tid] : 0.0;
+                    fy_ok = true;
+                } else {
+                    if (own) c.f[tid] = fyl;
+                    __syncthreads();
+                }
+                if (!inv_ok) {
+                    cta_build<float>(c, hf, A);
+                    cta_gj_invert(c, A);
+                }
+                if (cta_refine(c, A, hf, 8, 0.5, phase) != CTA_REFINE_OK) {
+                    st |= WIND_SYS_REFINE_FALLBACK;
+                    cta_mixed_pivoted_solve(c, hf, A);
+                }
+                y1l = own ? yl + hf * c.x[tid] : 0.0;
+                cta_build<float>(c, h1, A);
+                cta_gj_invert(c, A);
+                inv_ok = true;
+                if (cta_refine(c, A, h1, 24, 1.0, phase) != CTA_REFINE_OK) {
+                    st |= WIND_SYS_REFINE_FALLBACK;
+                    cta_mixed_pivoted_solve(c, h1, A);
+                    inv_ok = false;
+                }
+                const double vhl = own ? yl + h1 * c.x[tid] : 0.0;
+                if (own) c.v[tid] = vhl;
+                __syncthreads();
+                cta_rhs_fast(c);
+                int out = CTA_REFINE_GAVE_UP;
+                if (inv_ok) out = cta_refine(c, A, h2, 8, 0.0625, phase);
+                if (out != CTA_REFINE_OK) {
+                    cta_build<float>(c, h2, A);
+                    cta_gj_invert(c, A);
+                    inv_ok = false;
+                    if (cta_refine(c, A, h2, 24, 1.0, phase) != CTA_REFINE_OK) {
+                        st |= WIND_SYS_REFINE_FALLBACK;
+                        cta_mixed_pivoted_solve(c, h2, A);
+                    }
+                }
+                y2l = own ? vhl + h2 * c.x[tid] : 0.0;
+            } else
             for (int pass = 0; pass < 2; pass++) {
                 const int nsub = pass + 1;
                 if (own) c.v[tid] = yl;
@@ -900,6 +1201,7 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
                 h /= 2.0;
             } else {
                 unsolved = 0;
+                fy_ok = inv_ok = false;
                 if (own) yl = (METHOD == WIND_METHOD_RK2) ? (xd(2.0) * xd(y2l) - xd(y1l)).v : y2l;
                 if (tnow + h == tnow) { st |= WIND_SYS_STALLED; break; }
                 tnow += h;

@@ -51,7 +51,10 @@ wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, 
             gslot = std::max(gslot, lay.g_doubles);
         } else {
             const int nm = nmax_of(p.n_eq);
-            smem = std::max(smem, (size_t)(MIXED_THREADS / nm) * TeamLayout(nm, p.n_react, p.linear != nullptr, solver).bytes);
+            const bool reg = o.method == WIND_METHOD_SIE && solver != WIND_SOLVER_GJE_F64;
+            const size_t team_bytes = reg ? (size_t)WarpLayout(nm, p.n_react, p.linear != nullptr, solver).bytes
+                                          : (size_t)TeamLayout(nm, p.n_react, p.linear != nullptr, solver).bytes;
+            smem = std::max(smem, (size_t)(MIXED_THREADS / nm) * team_bytes);
         }
     }
     if (smem > (size_t)cap) return WIND_ERR_UNSUPPORTED;

@@ -36,7 +36,11 @@ static int team_blocks_per_sm(TeamFn fn, size_t smem) {
     return nb;
 }
 
+wind_status launch_warp(const wind_options& o, const KParams& p, cudaStream_t stream);
+
 wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream) {
+    // SIE with an LU or mixed solve: the register-resident kernel
+    if (o.method == WIND_METHOD_SIE && o.solver != WIND_SOLVER_GJE_F64) return launch_warp(o, p, stream);
     const int nmax = team_nmax(p.n_eq);
     TeamFn fn = nmax == 8 ? team_fn_8(o.method, o.controller, o.solver)
               : nmax == 16 ? team_fn_16(o.method, o.controller, o.solver)

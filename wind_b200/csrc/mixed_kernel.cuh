@@ -5,13 +5,15 @@
 // systems start earliest and the short ones fill the tail).  For each group
 // every block works on that group's device work queue -- one system per block
 // for N > 32 (cta_run), one system per team of 8/16/32 lanes for N <= 32
-// (team_run) -- until the queue is empty, then moves on to the next group.
+// (warp_run for SIE with the LU or mixed solve, team_run otherwise) -- until
+// the queue is empty, then moves on to the next group.
 // A block that finishes a group early starts the next one while others are
 // still on their last systems, so the groups overlap on the device.
 #pragma once
 
 #include "cta_kernel.cuh"
 #include "team_kernel.cuh"
+#include "warp_kernel.cuh"
 
 namespace wind {
 
@@ -25,10 +27,17 @@ __global__ void __launch_bounds__(MIXED_THREADS, 1)
     for (int gi = 0; gi < ngroups; gi++) {
         const KParams p = groups[order[gi]];
         if (p.nsys > 0) {
+            constexpr bool REG = METHOD == WIND_METHOD_SIE && SOLVER != WIND_SOLVER_GJE_F64;
             if (p.n_eq > 32) cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, gstride, smem_cap);
-            else if (p.n_eq > 16) team_run<32, METHOD, CTRL, SOLVER>(p, smem_raw);
-            else if (p.n_eq > 8) team_run<16, METHOD, CTRL, SOLVER>(p, smem_raw);
-            else team_run<8, METHOD, CTRL, SOLVER>(p, smem_raw);
+            else if constexpr (REG) {
+                if (p.n_eq > 16) warp_run<32, CTRL, SOLVER>(p, smem_raw);
+                else if (p.n_eq > 8) warp_run<16, CTRL, SOLVER>(p, smem_raw);
+                else warp_run<8, CTRL, SOLVER>(p, smem_raw);
+            } else {
+                if (p.n_eq > 16) team_run<32, METHOD, CTRL, SOLVER>(p, smem_raw);
+                else if (p.n_eq > 8) team_run<16, METHOD, CTRL, SOLVER>(p, smem_raw);
+                else team_run<8, METHOD, CTRL, SOLVER>(p, smem_raw);
+            }
         }
         __syncthreads();
     }

@@ -223,15 +223,44 @@ def workload_katz96(nsys: int = 65536, seed: int = 1, dt: float = 1e13,
     return Workload(net, y0, 0.0, dt, atol, rtol, 1, 1, "katz96")
 
 
+# Seeded synthetic batches are generated in chunks of CHUNK systems, chunk c
+# of a workload drawn from its own generator default_rng([seed, ..., c]), so
+# system i is the same whichever slice of the workload is asked for (a test
+# can take systems 0..63 of the 262,144-system batch without generating it).
+CHUNK = 4096
+
+
+def _chunked(nsys: int, first: int, make):
+    """Concatenate make(c) over the chunks covering [first, first + nsys)."""
+    c0, c1 = first // CHUNK, (first + nsys + CHUNK - 1) // CHUNK
+    parts = [make(c) for c in range(c0, max(c1, c0 + 1))]
+    lo = first - c0 * CHUNK
+    return parts, slice(lo, lo + nsys)
+
+
+def _cat_networks(nets, sl) -> Network:
+    n0 = nets[0]
+    cat = (lambda k: None if getattr(n0, k) is None
+           else np.ascontiguousarray(np.concatenate([getattr(n, k) for n in nets])[sl]))
+    rates, species, linear = cat("rates"), cat("species"), cat("linear")
+    return Network(n0.kind, n0.n_eq, int(rates.shape[0]), rates=rates, species=species,
+                   linear=linear)
+
+
 def workload_dense(nsys: int = 262144, seed: int = 2, n_eq: int = 32,
-                   n_react: int = 64) -> Workload:
+                   n_react: int = 64, first: int = 0) -> Workload:
     """Dense stiff network: L = Q diag(-lambda) Q^T with lambda log-U[1e-2,1e6]
     plus 64 random two-body reactions with k log-U[1e-3,1e1]; y0 U[0,1];
-    dt = 1, rtol 1e-6, atol 1e-8."""
-    rng = np.random.default_rng(seed)
-    net = random_mass_action(rng, nsys, n_eq, n_react, 1e-3, 1e1)
-    net.linear = dense_linear(rng, nsys, n_eq, 1e-2, 1e6)
-    y0 = rng.uniform(0.0, 1.0, size=(nsys, n_eq))
+    dt = 1, rtol 1e-6, atol 1e-8.  Systems [first, first + nsys) of the seeded
+    sequence (chunk c drawn from default_rng([seed, c]))."""
+    def make(c):
+        rng = np.random.default_rng([seed, c])
+        net = random_mass_action(rng, CHUNK, n_eq, n_react, 1e-3, 1e1)
+        net.linear = dense_linear(rng, CHUNK, n_eq, 1e-2, 1e6)
+        return net, rng.uniform(0.0, 1.0, size=(CHUNK, n_eq))
+    parts, sl = _chunked(nsys, first, make)
+    net = _cat_networks([p[0] for p in parts], sl)
+    y0 = np.ascontiguousarray(np.concatenate([p[1] for p in parts])[sl])
     return Workload(net, y0, 0.0, 1.0, 1e-8, 1e-6, 1, 1, f"dense_n{n_eq}")
 
 
@@ -239,20 +268,37 @@ MIXED_SIZES = (5, 16, 32, 64, 157)
 MIXED_FRACTIONS = (0.40, 0.25, 0.20, 0.10, 0.05)
 
 
-def workload_mixed(nsys: int = 200000, seed: int = 3, dt: float = 1e-2,
+def mixed_counts(nsys: int, fractions=MIXED_FRACTIONS) -> list:
+    """Systems per size class: rounded fractions, the last class takes the rest."""
+    counts = [int(round(nsys * f)) for f in fractions]
+    counts[-1] = nsys - sum(counts[:-1])
+    return counts
+
+
+def workload_mixed_class(n_eq: int, nsys: int, seed: int = 3, dt: float = 1.0,
+                         atol: float = 1e-8, rtol: float = 1e-6, first: int = 0) -> Workload:
+    """Systems [first, first + nsys) of the N = n_eq class of the mixed-size
+    batch: random two-body networks with 10N reactions, k log-U[1e-4,1e4],
+    y0 U[0,1] (chunk c drawn from default_rng([seed, n_eq, c]))."""
+    def make(c):
+        rng = np.random.default_rng([seed, n_eq, c])
+        net = random_mass_action(rng, CHUNK, n_eq, 10 * n_eq, 1e-4, 1e4)
+        return net, rng.uniform(0.0, 1.0, size=(CHUNK, n_eq))
+    parts, sl = _chunked(nsys, first, make)
+    net = _cat_networks([p[0] for p in parts], sl)
+    y0 = np.ascontiguousarray(np.concatenate([p[1] for p in parts])[sl])
+    return Workload(net, y0, 0.0, dt, atol, rtol, 1, 1, f"mixed_n{n_eq}")
+
+
+def workload_mixed(nsys: int = 200000, seed: int = 3, dt: float = 1.0,
                    atol: float = 1e-8, rtol: float = 1e-6,
                    sizes=MIXED_SIZES, fractions=MIXED_FRACTIONS) -> list:
     """Mixed-size batch: N in {5,16,32,64,157} at 40/25/20/10/5 %, each system
     a random two-body network with 10N reactions, k log-U[1e-4,1e4]; y0 U[0,1].
-    Returns one Workload per size class (counts from the fractions)."""
-    rng = np.random.default_rng(seed)
-    counts = [int(round(nsys * f)) for f in fractions]
-    counts[-1] = nsys - sum(counts[:-1])
+    Returns one Workload per size class (counts from the fractions); class N
+    holds the first systems of :func:`workload_mixed_class` for N."""
     out = []
-    for n_eq, cnt in zip(sizes, counts):
-        if cnt <= 0:
-            continue
-        net = random_mass_action(rng, cnt, n_eq, 10 * n_eq, 1e-4, 1e4)
-        y0 = rng.uniform(0.0, 1.0, size=(cnt, n_eq))
-        out.append(Workload(net, y0, 0.0, dt, atol, rtol, 1, 1, f"mixed_n{n_eq}"))
+    for n_eq, cnt in zip(sizes, mixed_counts(nsys, fractions)):
+        if cnt > 0:
+            out.append(workload_mixed_class(n_eq, cnt, seed, dt, atol, rtol))
     return out
