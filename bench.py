@@ -289,8 +289,6 @@ def run_main(args, wl, desc):
     nsteps = torch.zeros(S, dtype=torch.int64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
     bounds = slice_bounds(S, args.steps)
-    main_solver = args.solver if args.solver != "auto" else (
-        "mixed" if net.kind == W.NET_MASS_ACTION else "lu_f64")
 
     def launch(solver, s0, s1, timeout_s=0.0):
         """One wind_integrate launch over systems [s0, s1) of the resident
@@ -317,9 +315,26 @@ def run_main(args, wl, desc):
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) * 1e-3, n
 
-    # ---- warm-up: W slices of the main solver (untimed)
-    for i in range(args.warmup):
-        timed(main_solver, *bounds[i % len(bounds)])
+    # ---- warm-up (untimed): W launches of each fast solver on a few systems
+    b0 = bounds[0]
+    cand = ["mixed", "lu_f64"] if args.solver == "auto" else [args.solver]
+    for s in cand:
+        for i in range(args.warmup):
+            timed(s, b0[0], min(b0[1], b0[0] + 1024))
+
+    # ---- the same first systems with MIXED and LU_F64: the solver ratio, and
+    # (solver "auto") the headline solver = the faster one
+    cmp_hi = min(b0[1], b0[0] + args.compare_systems)
+    results, outs = {}, {}
+    for s in ("mixed", "lu_f64"):
+        t, n = timed(s, b0[0], cmp_hi)
+        outs[s] = y.cpu().numpy()[b0[0]:cmp_hi]
+        results[s] = {"systems_per_s": (cmp_hi - b0[0]) / t, "substeps": n,
+                      "systems": cmp_hi - b0[0], "timed": f"systems 0..{cmp_hi - 1}",
+                      "flagged_systems": int((status[b0[0]:cmp_hi].cpu().numpy() != 0).sum())}
+    mixed_over_fp64 = results["mixed"]["systems_per_s"] / results["lu_f64"]["systems_per_s"]
+    main_solver = args.solver if args.solver != "auto" else max(
+        cand, key=lambda s: results[s]["systems_per_s"])
 
     # ---- the timed job: every system once, K launches
     if dist is not None:
@@ -345,41 +360,19 @@ def run_main(args, wl, desc):
     y_main = y.cpu().numpy()
     st_main = status.cpu().numpy()
     steps_main = nsteps.cpu().numpy()
-    results = {main_solver: {"systems_per_s": S / sum(times), "substeps": substeps,
-                             "systems": S, "timed": "all slices",
-                             "flagged_systems": int((st_main != 0).sum())}}
+    results[main_solver + "_full_job"] = {"systems_per_s": S / sum(times), "substeps": substeps,
+                                          "systems": S, "timed": "all slices",
+                                          "flagged_systems": int((st_main != 0).sum())}
+    outs[main_solver] = y_main
 
-    # ---- the other solvers on slice 0 (LU) / under a deadline (GJE)
-    b0 = bounds[0]
-    outs = {main_solver: y_main}
-    for s in ("lu_f64", "mixed"):
-        if s == main_solver:
-            continue
-        timed(s, b0[0], min(b0[1], b0[0] + 2048))  # warm-up of this kernel
-        t, n = timed(s, *b0)
-        outs[s] = y.cpu().numpy()[b0[0]:b0[1]]
-        results[s] = {"systems_per_s": (b0[1] - b0[0]) / t, "substeps": n, "systems": b0[1] - b0[0],
-                      "timed": "slice 0"}
-    if "gje_f64" not in results:
-        t, n = timed("gje_f64", *b0, timeout_s=args.gje_seconds)
-        per_sys = float(steps_main[b0[0]:b0[1]].mean())
-        results["gje_f64"] = {"substeps_per_s": n / t, "systems_per_s": n / t / per_sys,
-                              "substeps": n, "timed": (f"slice 0 under a {args.gje_seconds:g} s device "
-                                                       "deadline; systems/s = substeps/s / mean "
-                                                       "substeps per system of the main run")}
-    # same-slice ratio (slice 0 of the main run vs LU_F64's slice 0)
-    t_main0 = times[0]
-    if "lu_f64" in results and main_solver != "lu_f64":
-        results["lu_f64"]["main_slice0_s"] = t_main0
-    mixed_over_fp64 = None
-    if "mixed" in results and "lu_f64" in results:
-        if main_solver == "mixed":
-            mixed_over_fp64 = (b0[1] - b0[0]) / t_main0 / results["lu_f64"]["systems_per_s"]
-        else:
-            mixed_over_fp64 = results["mixed"]["systems_per_s"] / (b0[1] - b0[0]) * t_main0
-    mixed_over_gje = None
-    if "mixed" in results:
-        mixed_over_gje = results["mixed"]["systems_per_s"] / results["gje_f64"]["systems_per_s"]
+    # ---- GJE_F64 (the reference's Gauss-Jordan in FP64): rate under a deadline
+    t, n = timed("gje_f64", *b0, timeout_s=args.gje_seconds)
+    per_sys = float(steps_main[b0[0]:b0[1]].mean())
+    results["gje_f64"] = {"substeps_per_s": n / t, "systems_per_s": n / t / per_sys,
+                          "substeps": n, "timed": (f"slice 0 under a {args.gje_seconds:g} s device "
+                                                   "deadline; systems/s = substeps/s / mean "
+                                                   "substeps per system of the main run")}
+    mixed_over_gje = results["mixed"]["systems_per_s"] / results["gje_f64"]["systems_per_s"]
 
     # ---- e2e through the C ABI with pinned host buffers (first slices)
     e2e_slices = bounds[:min(len(bounds), args.e2e_slices)]
@@ -455,7 +448,7 @@ def run_main(args, wl, desc):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         n_cpu = reference_sample_size(wl, args.method, args.ref_seconds, cores)
-        n_cpu = min(n_cpu, b0[1] - b0[0])
+        n_cpu = min(n_cpu, cmp_hi - b0[0])
         if n_cpu > 0:
             dt, y_ref = reference_run(wl, 0, n_cpu, args.method, cores)
             cpu = {"value": n_cpu / dt, "unit": "systems/s", "cores": cores, "kind": "reference",
@@ -484,7 +477,7 @@ def run_main(args, wl, desc):
             "data": "synthetic",
             "config": dict(config_dict(args, wl, desc), solver=main_solver),
             "solvers": results, "mixed_over_fp64": mixed_over_fp64,
-            "mixed_over_fp64_definition": "MIXED / LU_F64 systems/s, the same slice 0",
+            "mixed_over_fp64_definition": "MIXED / LU_F64 systems/s on the same first systems",
             "mixed_over_gje_f64": mixed_over_gje,
             "max_rel_err_vs_reference": errs or None,
             "e2e": {"value": world * e2e_sys / e2e_tot, "unit": "systems/s",
@@ -625,6 +618,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--gje-seconds", type=float, default=3.0)
     ap.add_argument("--e2e-slices", type=int, default=3)
+    ap.add_argument("--compare-systems", type=int, default=16384,
+                    help="systems of slice 0 integrated by both MIXED and LU_F64 for their ratio")
     ap.add_argument("--traffic-per-system", type=float, default=0.0,
                     help="DRAM bytes per system per launch from an ncu capture (roofline.traffic)")
     ap.add_argument("--profile", action="store_true",

@@ -186,6 +186,28 @@ int wind_integrate_batch(const wind_options* opt, const wind_group* groups,
 int wind_integrate_batch_noalloc(const wind_options* opt, const wind_group* groups,
                                  int32_t ngroups, void* stream);
 
+/* ---- the SIE_host variant: one step shared by every system -------------- */
+/* Replaces cudaIntegrateSIE (cuda/SIE_host/harness_kernel.cu:427-532, exported
+ * as _Z16cudaIntegrateSIEffiPfS_iiff, bound by python/wind_harness.py:27-28)
+ * and its controller errorLoop (:248-425): all nsys systems take the same
+ * step; an attempt (one full SIE substep and two half substeps from the last
+ * accepted state, 3 substeps counted per system) is refined for ALL systems
+ * when any element of any system fails the SIE_host error test
+ * (vector_kernels.cu:45-70: |y1-y2| > atol, or |(y1-y2)/(y2+1e-12)| > rtol
+ * with y1 > atol and y2 > atol -- strict and signed); an accepted attempt
+ * takes y2 for all systems and doubles the step.  The loop stops at tend or
+ * after 9 consecutive refinements, leaving the last accepted state;
+ * *t_reached (may be null) receives the time reached, *total_nsteps the
+ * reference's return value (substeps per system times nsys).  Compiled
+ * networks only (NR_test, Katz96, StiffTrig; mass action returns
+ * WIND_ERR_UNSUPPORTED), SIE only; opt->solver selects the linear solve
+ * (GJE_F64 is the reference's Gauss-Jordan in FP64), opt->controller is not
+ * used.  Host or device memory as in wind_integrate. */
+int wind_integrate_global(const wind_options* opt, const wind_network* net, double tnow,
+                          double tend, int32_t n_integration_steps, double* y, int64_t nsys,
+                          double atol, double rtol, int64_t* total_nsteps, double* t_reached,
+                          int32_t memory, void* stream);
+
 /* ---- device-resident output loop (the caller loop of
  * python/ode_systems/ode_base.py:315-397) -------------------------------- */
 /* Integrate n_output_steps intervals of (tend-tnow)/n_output_steps each, with

@@ -21,6 +21,17 @@
 int cudaIntegrateSystem(float tnow, float tend, int n_integration_steps,
                         float* constants, float* equations, int Nsystems,
                         int Nequations_per_system, float ABSOLUTE, float RELATIVE);
+
+/* Replaces cudaIntegrateSIE of cuda/SIE_host/harness_kernel.cu:427-532
+ * (exported mangled as _Z16cudaIntegrateSIEffiPfS_iiff, looked up by
+ * python/wind_harness.py:27-28), built into wind_b200/lib/<network>/sie_host.so
+ * like the reference's lib/sie_host.so: the same arguments as
+ * cudaIntegrateSystem, one step shared by all systems (wind_integrate_global
+ * in wind.h), returns the substep count per system times Nsystems, or -1 on
+ * a CUDA failure. */
+int cudaIntegrateSIE(float tnow, float tend, int n_integration_steps, float* constants,
+                     float* equations, int Nsystems, int Neqn_p_sys, float ABSOLUTE,
+                     float RELATIVE);
 #endif
 
 #endif /* WIND_LEGACY_H */

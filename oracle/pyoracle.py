@@ -44,6 +44,10 @@ def _load_oracle():
             C.c_int, C.c_int, C.POINTER(_capi.WindNetwork), C.c_double, C.c_double,
             C.c_int, P, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int64, P, P]
         lib.wind_oracle_integrate.restype = C.c_int64
+        lib.wind_oracle_integrate_global.argtypes = [
+            C.POINTER(_capi.WindNetwork), C.c_double, C.c_double, C.c_int, P, C.c_int64,
+            C.c_double, C.c_double, C.POINTER(C.c_double)]
+        lib.wind_oracle_integrate_global.restype = C.c_int64
         lib.wind_oracle_rhs_jac.argtypes = [C.POINTER(_capi.WindNetwork), C.c_int64,
                                             P, P, P]
         lib.wind_oracle_rhs_jac.restype = C.c_int
@@ -88,6 +92,21 @@ def restated(net: Network, y: np.ndarray, tnow: float, tend: float, atol: float,
     if any(t < 0 for t in tot):
         raise ValueError("oracle rejected the arguments")
     return int(sum(tot)), status, steps
+
+
+def restated_global(net: Network, y: np.ndarray, tnow: float, tend: float, atol: float,
+                    rtol: float, n_integration_steps: int = 1):
+    """The SIE_host controller restated (one step shared by all systems);
+    updates ``y`` in place, returns (total substeps, time reached)."""
+    lib = _load_oracle()
+    assert y.dtype == np.float64 and y.flags["C_CONTIGUOUS"]
+    ns = _capi.network_struct(net)
+    t = C.c_double(0.0)
+    tot = lib.wind_oracle_integrate_global(C.byref(ns), tnow, tend, n_integration_steps,
+                                           y.ctypes.data, net.nsys, atol, rtol, C.byref(t))
+    if tot < 0:
+        raise ValueError("oracle rejected the arguments")
+    return int(tot), float(t.value)
 
 
 def rhs_jac(net: Network, s: int, y: np.ndarray):

@@ -374,3 +374,64 @@ int wind_oracle_sie_substep(const wind_network* net, int64_t s, int ctrl,
     free(w);
     return 0;
 }
+
+/* The SIE_host variant's controller (cuda/SIE_host/harness_kernel.cu:248-425,
+ * errorLoop): every system advances with ONE shared step.  Per attempt
+ * (3 substeps counted per system, :292): y1 = one substep of h, y2 = two of
+ * h/2 from the last accepted state (solveSystem, :175-246, with GOLD
+ * substep arithmetic: h_sub = (t1 - t0)/n, y += h*(Inv f)); the error flag is
+ * set when ANY element of ANY system fails checkError (vector_kernels.cu:45-70:
+ * |y1 - y2| > atol, or |(y1 - y2)/(y2 + 1e-12)| > rtol with y1 > atol and
+ * y2 > atol -- signed, strict).  A failed attempt halves the step for all
+ * (:363-367); an accepted one takes y2 for all, advances t and doubles the
+ * step (:383-400).  The loop ends at tend or after 9 consecutive refinements
+ * (:289), leaving the last accepted state.  Returns the substep total over
+ * all systems (nsteps * Nsystems, :423), *t_reached the time reached. */
+int64_t wind_oracle_integrate_global(const wind_network* net, double tnow, double tend,
+                                     int n_integration_steps, double* y, int64_t nsys,
+                                     double atol, double rtol, double* t_reached) {
+    if (!net || !y || net->n_eq < 1 || net->n_eq > ORACLE_MAXN || n_integration_steps < 1 ||
+        nsys < 0)
+        return -1;
+    int n = net->n_eq;
+    scratch_t* w = (scratch_t*)malloc(sizeof(scratch_t));
+    double* y1 = (double*)malloc(sizeof(double) * (size_t)(nsys > 0 ? nsys : 1) * n);
+    double* y2 = (double*)malloc(sizeof(double) * (size_t)(nsys > 0 ? nsys : 1) * n);
+    if (!w || !y1 || !y2) { free(w); free(y1); free(y2); return -1; }
+    int64_t nsteps = 0;
+    int unsolved = 0;
+    double timestep = (tend - tnow) / n_integration_steps;
+    while (tnow < tend && unsolved < 9) {
+        timestep = fmin(timestep, tend - tnow);
+        nsteps += 3;
+        int flag = 0;
+        for (int64_t s = 0; s < nsys; s++) {
+            sysref sr = {net, s};
+            double* a = y1 + s * n;
+            double* b = y2 + s * n;
+            memcpy(a, y + s * n, sizeof(double) * n);
+            memcpy(b, y + s * n, sizeof(double) * n);
+            take_step(&sr, WIND_METHOD_SIE, WIND_CTRL_GOLD, tnow, tnow + timestep, 1, a, w);
+            take_step(&sr, WIND_METHOD_SIE, WIND_CTRL_GOLD, tnow, tnow + timestep, 2, b, w);
+            for (int e = 0; e < n; e++) {
+                if (fabs(a[e] - b[e]) > atol) flag = 1;
+                if (fabs((a[e] - b[e]) / (b[e] + 1e-12)) > rtol && a[e] > atol && b[e] > atol)
+                    flag = 1;
+            }
+        }
+        if (flag) {
+            unsolved++;
+            timestep /= 2;
+        } else {
+            unsolved = 0;
+            memcpy(y, y2, sizeof(double) * (size_t)nsys * n);
+            tnow += timestep;
+            timestep *= 2;
+        }
+    }
+    if (t_reached) *t_reached = tnow;
+    free(w);
+    free(y1);
+    free(y2);
+    return nsteps * nsys;
+}

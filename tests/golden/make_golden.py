@@ -2,7 +2,7 @@
 (cuda/c_baseline, compiled from the reference sources by oracle/build_ref.sh
 in FP64 with -Dfloat=double) run on small seeded inputs of every network.
 
-    python tests/golden/make_golden.py      # needs oracle/_ref built
+    WIND_REFERENCE=<reference checkout> python tests/golden/make_golden.py   # needs oracle/_ref built
 
 Writes tests/golden/golden.npz.  Each case stores the inputs (network arrays,
 y0, interval, tolerances) and the reference outputs (final state, total
@@ -22,7 +22,11 @@ from oracle import pyoracle as O  # noqa: E402
 from wind_b200 import networks as W  # noqa: E402
 
 
-def reference_fixture(path="/root/reference/cuda/debug/inputKatz96_1_1_1.h"):
+REFERENCE = os.environ.get("WIND_REFERENCE", "")
+FIXTURE = os.path.join(REFERENCE, "cuda", "debug", "inputKatz96_1_1_1.h")
+
+
+def reference_fixture(path=FIXTURE):
     """The reference's committed debug input (4 Katz96 cells), parsed from the
     header its dlopen driver includes (cuda/debug/debug.c:1); the driver runs
     it with tend = 10 and abs = rel = 5e-3 (debug.c:19,29-30)."""
@@ -41,7 +45,7 @@ def reference_fixture(path="/root/reference/cuda/debug/inputKatz96_1_1_1.h"):
 
 def cases():
     out = []
-    if os.path.exists("/root/reference/cuda/debug/inputKatz96_1_1_1.h"):
+    if REFERENCE and os.path.exists(FIXTURE):
         fx = reference_fixture()
         out.append(("fixture_katz96_debug_sie", "sie", fx))
         out.append(("fixture_katz96_debug_rk2", "rk2", fx))

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _declared(header):
     src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(wind_\w+|cudaIntegrateSystem)\s*\(",
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(wind_\w+|cudaIntegrate\w+)\s*\(",
                                  src, flags=re.M)))
 
 
@@ -31,9 +31,41 @@ def test_libwind_exports_every_declared_symbol():
 @pytest.mark.parametrize("net", ["nr_test", "katz96", "stifftrig"])
 @pytest.mark.parametrize("method", ["sie", "rk2"])
 def test_legacy_libraries_export_reference_symbol(net, method):
-    assert _declared("wind_legacy.h") == ["cudaIntegrateSystem"]
+    assert _declared("wind_legacy.h") == ["cudaIntegrateSIE", "cudaIntegrateSystem"]
     fn = lib.legacy(net, method)  # looks up _Z19cudaIntegrateSystemffiPfS_iiff
     assert fn is not None
+
+
+@pytest.mark.parametrize("net", ["nr_test", "katz96", "stifftrig"])
+def test_sie_host_libraries_export_reference_symbol(net):
+    fn = lib.legacy_host(net)  # looks up _Z16cudaIntegrateSIEffiPfS_iiff
+    assert fn is not None
+
+
+def test_global_entry_argument_errors():
+    w = lib.load()
+    wl = W.workload_mixed_class(5, 2, dt=1e-3)
+    ns = _capi.network_struct(wl.net)
+    y = wl.y0.copy()
+    o = lib.options("sie", "gje_f64", "gold")
+    tot, t = C.c_int64(0), C.c_double(0.0)
+    # mass action is outside the SIE_host variant's scope
+    assert w.wind_integrate_global(C.byref(o), C.byref(ns), 0.0, 1e-3, 1, y.ctypes.data, 2, 1e-8,
+                                   1e-6, C.byref(tot), C.byref(t), _capi.MEM_HOST,
+                                   None) == _capi.WIND_ERR_UNSUPPORTED
+    k = W.workload_katz96(2)
+    ks = _capi.network_struct(k.net)
+    yk = k.y0.copy()
+    for bad in (dict(method=_capi.METHODS["rk2"]), dict(solver=7)):
+        ob = lib.options("sie", "gje_f64", "gold")
+        for f, v in bad.items():
+            setattr(ob, f, v)
+        assert w.wind_integrate_global(C.byref(ob), C.byref(ks), 0.0, 1.0, 1, yk.ctypes.data, 2,
+                                       1e-8, 1e-6, C.byref(tot), C.byref(t), _capi.MEM_HOST,
+                                       None) == _capi.WIND_ERR_ARGUMENT
+    assert w.wind_integrate_global(C.byref(o), C.byref(ks), 0.0, 1.0, 0, yk.ctypes.data, 2, 1e-8,
+                                   1e-6, C.byref(tot), C.byref(t), _capi.MEM_HOST,
+                                   None) == _capi.WIND_ERR_ARGUMENT
 
 
 def test_defaults_and_strings():

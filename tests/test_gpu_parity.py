@@ -176,17 +176,22 @@ def test_mixed_size_single_launch(cuda_device, solver):
 
 
 def test_cta_mixed_fallback_flag(cuda_device):
-    """MIXED factors N > 32 systems without pivoting; a first full step whose
-    (I - hJ)[0][0] is ~0 cannot be refined, the substep is redone with
-    partial pivoting and the system carries WIND_SYS_REFINE_FALLBACK, with
-    the result of the FP64 LU path."""
+    """MIXED inverts N > 32 systems by Gauss-Jordan without pivoting.  Here
+    (I - hJ)[0][0] of the first full step is exactly zero (no reaction
+    touches species 0 and h L[0][0] = 1), so the inverse cannot be formed:
+    the substep is redone with the partial-pivoting LU, the system carries
+    WIND_SYS_REFINE_FALLBACK, and its result is the FP64 LU path's.  Species
+    0 and 1 are coupled through L so the matrix stays nonsingular."""
     rng = np.random.default_rng(7)
     n, s, dt = 40, 4, 1e-3
-    net = W.random_mass_action(rng, s, n, 80, 1e-3, 1e-1)
+    net = W.random_mass_action(rng, s, n - 1, 80, 1e-3, 1e-1)
+    net.species = (net.species + 1).astype(np.uint16)  # species 1..N-1 only
+    net.n_eq = n
     lin = np.zeros((s, n, n), np.float32)
     for k in range(s):
         lin[k] = -np.eye(n, dtype=np.float32)
-        lin[k, 0, 0] = np.float32(1.0 / dt) * (1.0 + 1e-7 * k)
+        lin[k, 0, 0] = np.float32(1.0 / dt)
+        lin[k, 0, 1] = lin[k, 1, 0] = np.float32(1.0)
     net.linear = lin
     y0 = rng.uniform(0.5, 1.0, (s, n))
     y_lu, y_mx = y0.copy(), y0.copy()
@@ -194,6 +199,6 @@ def test_cta_mixed_fallback_flag(cuda_device):
     _, st_mx, _ = lib.integrate(net, y_mx, 0.0, dt, 1e-8, 1e-6, "sie", "mixed", "device")
     st_lu, st_mx = np.asarray(st_lu), np.asarray(st_mx)
     assert not (st_lu & 8).any()
-    assert st_mx[0] & 8
+    assert (st_mx & 8).all()
     assert np.isfinite(y_mx).all()
     assert mixed_err(y_mx, y_lu, 1e-8) <= 1e-5

@@ -110,3 +110,37 @@ def test_oracle_edge_cases():
     y[1, 0] = np.nan
     tot, st, _ = O.restated(wl.net, y, 0.0, 1e10, 1e-3, 1e-3)
     assert st[1] & 1 and st[0] == 0
+
+
+def test_global_controller_nr_known_answer():
+    """The SIE_host controller (one step shared by all systems) restated.  It
+    gives up after 9 consecutive refinements, so its callers start from a
+    small step: with 1000 initial steps per output interval the NR test over
+    t = 0..1 in 100 intervals reaches every interval's end and tracks the
+    exact solution (first-order SIE at rtol 1e-6); every attempt counts 3
+    substeps per system."""
+    wl = W.workload_nr(64)
+    y = wl.y0.copy()
+    dt = (wl.tend - wl.tnow) / wl.n_output_steps
+    total = 0
+    for k in range(wl.n_output_steps):
+        tot, t_reached = O.restated_global(wl.net, y, wl.tnow + k * dt, wl.tnow + (k + 1) * dt,
+                                           wl.atol, wl.rtol, 1000)
+        assert t_reached >= wl.tnow + (k + 1) * dt * (1 - 1e-12)
+        assert tot % (3 * wl.net.nsys) == 0
+        total += tot
+    exact = W.nr_analytic(wl.y0, wl.tend)
+    assert np.max(np.abs(y - exact) / np.abs(exact)) < 1e-4
+    assert total > 0
+
+
+def test_global_controller_gives_up_after_nine_refinements():
+    """With a tolerance no step can meet, the shared-step loop stops after 9
+    consecutive refinements (harness_kernel.cu:289): 10 attempts, the state
+    untouched and the time not advanced."""
+    wl = W.workload_katz96(4, seed=12)
+    y = wl.y0.copy()
+    tot, t_reached = O.restated_global(wl.net, y, 0.0, 1e13, 1e-30, 1e-30)
+    assert t_reached == 0.0
+    assert np.array_equal(y, wl.y0)
+    assert tot == 9 * 3 * 4

@@ -132,6 +132,10 @@ def declare_api(lib: C.CDLL) -> C.CDLL:
         C.c_int32, C.c_int32, P, C.c_int64, C.c_double, C.c_double, P, P,
         C.c_int32, P]
     lib.wind_integrate_output_steps.restype = C.c_int
+    lib.wind_integrate_global.argtypes = [
+        C.POINTER(WindOptions), C.POINTER(WindNetwork), C.c_double, C.c_double,
+        C.c_int32, P, C.c_int64, C.c_double, C.c_double, P, P, C.c_int32, P]
+    lib.wind_integrate_global.restype = C.c_int
     lib.wind_version.restype = C.c_char_p
     lib.wind_status_string.argtypes = [C.c_int]
     lib.wind_status_string.restype = C.c_char_p

@@ -28,7 +28,7 @@ FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 
 # translation units of libwind.so
 UNITS = ["api", "batch", "noalloc", "dispatch_lane", "dispatch_team", "dispatch_team8",
-         "dispatch_team16", "dispatch_team32", "dispatch_warp", "dispatch_cta", "dispatch_mixed", "server"]
+         "dispatch_team16", "dispatch_team32", "dispatch_warp", "dispatch_cta", "dispatch_mixed", "server", "global"]
 
 LEGACY_NETS = {"nr_test": "WIND_NET_NR_TEST", "katz96": "WIND_NET_KATZ96",
                "stifftrig": "WIND_NET_STIFFTRIG"}
@@ -95,31 +95,33 @@ def build_native(verbose=False):
         _run([NVCC] + ARCH + ["-shared"] + objs + ["-o", libwind, "-lcudart"])
     for net, netdef in LEGACY_NETS.items():
         os.makedirs(os.path.join(LIB, net), exist_ok=True)
-        for meth, mdef in LEGACY_METHODS.items():
+        # sie.so / rk2.so export cudaIntegrateSystem; sie_host.so exports
+        # cudaIntegrateSIE (the reference's lib/sie_host.so)
+        for meth, mdef in list(LEGACY_METHODS.items()) + [("sie_host", "WIND_METHOD_SIE")]:
             out = os.path.join(LIB, net, f"{meth}.so")
             if _stale(out, deps + [libwind]):
+                extra = ["-DWIND_LEGACY_HOST"] if meth == "sie_host" else []
                 _run([NVCC] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-                      f"-DWIND_LEGACY_NET={netdef}", f"-DWIND_LEGACY_METHOD={mdef}",
-                      os.path.join(CSRC, "legacy.cu"), "-o", out,
+                      f"-DWIND_LEGACY_NET={netdef}", f"-DWIND_LEGACY_METHOD={mdef}"] + extra +
+                     [os.path.join(CSRC, "legacy.cu"), "-o", out,
                       "-L" + LIB, "-lwind", "-Xlinker", "-rpath=$ORIGIN/.."])
     return libwind
 
 
-def build_oracle(reference_dir="/root/reference"):
+def build_oracle():
     """The CPU checkers: the restatement always; the reference's own
-    c_baseline only when the reference sources are present."""
+    c_baseline through oracle/build_ref.sh, which locates the reference
+    checkout (WIND_REFERENCE) and exits 3 when its sources are absent -- then
+    only the restatement is built."""
     oracle = os.path.join(ROOT, "oracle")
     _run(["make", "-s", "-C", oracle])
-    if os.path.isdir(os.path.join(reference_dir, "cuda", "c_baseline")):
-        stamp = os.path.join(oracle, "_ref", "sie_gold_katz96_f64.so")
-        srcs = glob.glob(os.path.join(oracle, "plugins", "*.c")) + [os.path.join(oracle, "build_ref.sh")]
-        if _stale(stamp, srcs):
-            env = dict(os.environ, WIND_REFERENCE=reference_dir)
-            r = subprocess.run(["bash", os.path.join(oracle, "build_ref.sh")], env=env,
-                               capture_output=True, text=True)
-            if r.returncode != 0:
-                sys.stderr.write(r.stdout + r.stderr)
-                raise RuntimeError("oracle/build_ref.sh failed")
+    stamp = os.path.join(oracle, "_ref", "sie_gold_katz96_f64.so")
+    srcs = glob.glob(os.path.join(oracle, "plugins", "*.c")) + [os.path.join(oracle, "build_ref.sh")]
+    if _stale(stamp, srcs):
+        r = subprocess.run(["bash", os.path.join(oracle, "build_ref.sh")], capture_output=True, text=True)
+        if r.returncode not in (0, 3):
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("oracle/build_ref.sh failed")
 
 
 def main():

@@ -38,6 +38,10 @@ struct CtaPlan {
 };
 wind_status plan_cta(const wind_options& o, const KParams& p, bool allow_global, CtaPlan* out);
 wind_status launch_cta(const CtaPlan& pl, const KParams& p, cudaStream_t stream, double* scratch);
+// Global scratch (bytes) one resident CTA-kernel block needs for an N > 32
+// mass-action system with the full shared-memory budget (0 when everything
+// fits in shared memory).
+size_t cta_scratch_bytes_per_block(int n_eq, int n_react, bool lin, int solver);
 extern std::atomic<int64_t> g_launches;
 // Largest N any kernel family accepts (lane/team kernels up to 32, CTA
 // kernels up to 256).

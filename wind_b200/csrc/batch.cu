@@ -12,6 +12,45 @@ namespace wind {
 
 wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, cudaStream_t stream);
 
+// Streams and events for the builtin groups that run beside the mass-action
+// launch, kept per host thread and device and reused by every call (a
+// request loop calls launch_batch once per batch: creating and destroying
+// them each time would sit on its latency path).  They live until the
+// process exits.
+struct ForkPool {
+    int device = -1;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> done;
+};
+
+static wind_status fork_pool(size_t n, ForkPool** out) {
+    thread_local std::vector<ForkPool> pools;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return launch_status("fork pool device");
+    ForkPool* fp = nullptr;
+    for (auto& p : pools)
+        if (p.device == dev) fp = &p;
+    if (!fp) {
+        pools.emplace_back();
+        fp = &pools.back();
+        fp->device = dev;
+        if (cudaEventCreateWithFlags(&fp->fork, cudaEventDisableTiming) != cudaSuccess)
+            return launch_status("fork event");
+    }
+    while (fp->streams.size() < n) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+            return launch_status("fork stream");
+        fp->streams.push_back(st);
+        fp->done.push_back(ev);
+    }
+    *out = fp;
+    return WIND_OK;
+}
+
 wind_status launch_batch(const wind_options& o, const wind_group* groups, int ngroups,
                          cudaStream_t stream) {
     for (int g = 0; g < ngroups; g++) {
@@ -59,29 +98,20 @@ wind_status launch_batch(const wind_options& o, const wind_group* groups, int ng
         (p.kind == WIND_NET_MASS_ACTION ? mass : builtin).push_back(p);
     }
     wind_status st = WIND_OK;
-    cudaEvent_t fork = nullptr;
-    std::vector<cudaStream_t> ss(builtin.size(), nullptr);
-    std::vector<cudaEvent_t> done(builtin.size(), nullptr);
+    ForkPool* fp = nullptr;
     if (!builtin.empty()) {
-        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
-        cudaEventRecord(fork, stream);
+        st = fork_pool(builtin.size(), &fp);
+        if (st == WIND_OK) st = cuda_status(cudaEventRecord(fp->fork, stream), "fork record");
     }
     for (size_t g = 0; g < builtin.size() && st == WIND_OK; g++) {
-        cudaStreamCreateWithFlags(&ss[g], cudaStreamNonBlocking);
-        cudaEventCreateWithFlags(&done[g], cudaEventDisableTiming);
-        cudaStreamWaitEvent(ss[g], fork, 0);
-        st = launch_integrate(o, builtin[g], ss[g]);
-        cudaEventRecord(done[g], ss[g]);
+        cudaStreamWaitEvent(fp->streams[g], fp->fork, 0);
+        st = launch_integrate(o, builtin[g], fp->streams[g]);
+        cudaEventRecord(fp->done[g], fp->streams[g]);
     }
     if (st == WIND_OK) st = launch_mixed(o, mass, stream);
-    for (size_t g = 0; g < builtin.size(); g++)
-        if (done[g]) cudaStreamWaitEvent(stream, done[g], 0);
+    if (fp)
+        for (size_t g = 0; g < builtin.size(); g++) cudaStreamWaitEvent(stream, fp->done[g], 0);
     cudaFreeAsync(counters, stream);
-    for (size_t g = 0; g < builtin.size(); g++) {
-        if (ss[g]) cudaStreamDestroy(ss[g]);
-        if (done[g]) cudaEventDestroy(done[g]);
-    }
-    if (fork) cudaEventDestroy(fork);
     return st;
 }
 

@@ -102,6 +102,11 @@ wind_status plan_cta(const wind_options& o, const KParams& p, bool allow_global,
     return WIND_OK;
 }
 
+size_t cta_scratch_bytes_per_block(int n_eq, int n_react, bool lin, int solver) {
+    const CtaLayout lay(n_eq, n_react, lin, solver, smem_optin());
+    return lay.g_doubles * sizeof(double);
+}
+
 wind_status launch_cta(const CtaPlan& pl, const KParams& p, cudaStream_t stream, double* scratch) {
     if (pl.gstride && !scratch) return WIND_ERR_ARGUMENT;
     CtaFn fn = reinterpret_cast<CtaFn>(const_cast<void*>(pl.fn));

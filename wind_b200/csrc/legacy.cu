@@ -38,6 +38,37 @@ static int legacy_n_const(int kind) {
     return kind == WIND_NET_KATZ96 ? 10 : (kind == WIND_NET_NR_TEST ? 4 : 2);
 }
 
+#ifdef WIND_LEGACY_HOST
+// The SIE_host library: cudaIntegrateSIE with the shared-step controller.
+int cudaIntegrateSIE(float tnow, float tend, int n_integration_steps, float* constants,
+                     float* equations, int Nsystems, int Neqn_p_sys, float ABSOLUTE, float RELATIVE) {
+    if (Nsystems <= 0) return 0;
+    const int N = Neqn_p_sys;
+    const int nc = legacy_n_const(WIND_LEGACY_NET);
+    std::vector<double> c((size_t)Nsystems * nc), y((size_t)Nsystems * N);
+    for (size_t i = 0; i < c.size(); i++) c[i] = constants[i];
+    for (size_t i = 0; i < y.size(); i++) y[i] = equations[i];
+    wind_network net;
+    std::memset(&net, 0, sizeof(net));
+    net.kind = WIND_LEGACY_NET;
+    net.n_eq = N;
+    net.n_const = nc;
+    net.constants = c.data();
+    wind_options o;
+    wind_default_options(&o);
+    if (const char* s = std::getenv("WIND_LEGACY_SOLVER")) {
+        if (!std::strcmp(s, "lu_f64")) o.solver = WIND_SOLVER_LU_F64;
+        else if (!std::strcmp(s, "mixed")) o.solver = WIND_SOLVER_MIXED;
+    }
+    int64_t total = 0;
+    const int st = wind_integrate_global(&o, &net, (double)tnow, (double)tend, n_integration_steps,
+                                         y.data(), Nsystems, (double)ABSOLUTE, (double)RELATIVE,
+                                         &total, nullptr, WIND_MEM_HOST, nullptr);
+    if (st != WIND_OK) return -1;
+    for (size_t i = 0; i < y.size(); i++) equations[i] = (float)y[i];
+    return (int)total;
+}
+#else
 int cudaIntegrateSystem(float tnow, float tend, int n_integration_steps, float* constants,
                         float* equations, int Nsystems, int Nequations_per_system,
                         float ABSOLUTE, float RELATIVE) {
@@ -70,3 +101,4 @@ int cudaIntegrateSystem(float tnow, float tend, int n_integration_steps, float* 
     for (size_t i = 0; i < y.size(); i++) equations[i] = (float)y[i];
     return (int)total;
 }
+#endif

@@ -19,8 +19,11 @@ namespace wind {
 
 constexpr int MIXED_THREADS = CTA_THREADS;
 
+// Two blocks per SM (128 registers) for the LU and mixed solvers, whose team
+// and CTA paths fit that budget; the reference Gauss-Jordan keeps a row of M
+// and of the inverse per lane in registers and gets the whole file.
 template <int METHOD, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(MIXED_THREADS, 1)
+__global__ void __launch_bounds__(MIXED_THREADS, SOLVER == WIND_SOLVER_GJE_F64 ? 1 : 2)
     k_mixed(const KParams* __restrict__ groups, const int* __restrict__ order, int ngroups,
             double* gscratch, size_t gstride, int smem_cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -82,9 +82,21 @@ struct Server {
     int worker_error = WIND_OK;
 };
 
-static size_t footprint(const ServerRequest& r) {
-    return r.nsys * (size_t)r.N * 8 + r.constants.size() * 8 + r.rates.size() * 8 +
-           r.species.size() * 2 + r.linear.size() * 4 + r.nsys * 12 + 64 * 8;
+// Device bytes a request holds while admitted: its state, network, status
+// and step counters, and -- for mass action with N > 32 -- the per-block
+// global scratch the CTA kernels take for what does not fit in shared
+// memory (one slot per resident block: up to two blocks per SM), counted
+// in full for every such request since each launch sizes it for its
+// largest group.
+static size_t footprint(const ServerRequest& r, const wind_server_config& cfg) {
+    size_t b = r.nsys * (size_t)r.N * 8 + r.constants.size() * 8 + r.rates.size() * 8 +
+               r.species.size() * 2 + r.linear.size() * 4 + r.nsys * 12 + 64 * 8;
+    if (r.kind == WIND_NET_MASS_ACTION && r.N > wind::WIND_TEAM_MAX_EQ) {
+        const int solver = (cfg.method == WIND_METHOD_RK2) ? WIND_SOLVER_LU_F64 : cfg.solver;
+        b += wind::cta_scratch_bytes_per_block(r.N, r.n_react, !r.linear.empty(), solver) *
+             (size_t)wind::device_sm_count() * 2;
+    }
+    return b;
 }
 
 // Upload inputs and allocate outputs on `s` (stream-ordered pool).
@@ -313,7 +325,7 @@ int wind_server_submit(wind_server* srv, const wind_request* q, int64_t* id_out)
             if (v >= r->N) { delete r; return WIND_ERR_ARGUMENT; }
     }
     if (q->net.linear) r->linear.assign(q->net.linear, q->net.linear + q->nsys * (size_t)r->N * r->N);
-    r->footprint = footprint(*r);
+    r->footprint = footprint(*r, S->cfg);
     // pinned result buffers, taken in the caller's thread so the worker's
     // launch path stays free of host allocations
     if (cudaMallocHost((void**)&r->h_y, r->nsys * (size_t)r->N * sizeof(double)) != cudaSuccess ||

@@ -150,6 +150,37 @@ def integrate_output_steps(net: Network, y: np.ndarray, tnow: float, tend: float
     return out, steps
 
 
+def integrate_global(net: Network, y: np.ndarray, tnow: float, tend: float, atol: float,
+                     rtol: float, solver: str = "gje_f64", n_integration_steps: int = 1):
+    """The SIE_host variant (cuda/SIE_host/harness_kernel.cu:248-425): one
+    step shared by all systems, refined for all when any system fails.
+    ``y`` (host float64 [S, N]) is updated in place; returns
+    ``(total_substeps, t_reached)``."""
+    lib = load()
+    assert isinstance(y, np.ndarray) and y.dtype == np.float64 and y.flags["C_CONTIGUOUS"]
+    o = options("sie", solver, "gold")
+    ns = _capi.network_struct(net)
+    total, t_reached = C.c_int64(0), C.c_double(0.0)
+    code = lib.wind_integrate_global(C.byref(o), C.byref(ns), tnow, tend, n_integration_steps,
+                                     y.ctypes.data, net.nsys, atol, rtol, C.byref(total),
+                                     C.byref(t_reached), _capi.MEM_HOST, None)
+    _check(code, "wind_integrate_global")
+    return int(total.value), float(t_reached.value)
+
+
+def legacy_host(network: str):
+    """The drop-in ``cudaIntegrateSIE`` of ``lib/<network>/sie_host.so``, bound
+    by the reference's mangled name (python/wind_harness.py:27-28)."""
+    path = os.path.join(LIBDIR, network, "sie_host.so")
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built")
+    fn = getattr(C.CDLL(path), "_Z16cudaIntegrateSIEffiPfS_iiff")
+    fn.argtypes = [C.c_float, C.c_float, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                   C.c_float, C.c_float]
+    fn.restype = C.c_int
+    return fn
+
+
 class DeviceGroup:
     """One workload's arrays on the device, kept alive for a batch call."""
 
