@@ -252,6 +252,17 @@ def run_reference_arm(args, wl, desc):
     print(json.dumps(line), flush=True)
 
 
+STATUS_BITS = {1: "nonfinite", 2: "max_attempts", 4: "stalled", 8: "refine_fallback",
+               16: "timeout", 32: "bad_input"}
+
+
+def status_counts(st) -> dict:
+    """Systems carrying each per-system status bit (include/wind.h)."""
+    st = np.asarray(st)
+    return {name: int(((st & bit) != 0).sum()) for bit, name in STATUS_BITS.items()
+            if ((st & bit) != 0).any()}
+
+
 def config_dict(args, wl, desc):
     return {"workload": desc, "method": args.method, "controller": args.controller,
             "systems": wl.net.nsys, "equations": wl.net.n_eq,
@@ -322,19 +333,17 @@ def run_main(args, wl, desc):
         for i in range(args.warmup):
             timed(s, b0[0], min(b0[1], b0[0] + 1024))
 
-    # ---- the same first systems with MIXED and LU_F64: the solver ratio, and
+    # ---- MIXED vs LU_F64 on the same first slice under the same device
+    # deadline: substeps/s of each at full occupancy (the ratio), and
     # (solver "auto") the headline solver = the faster one
-    cmp_hi = min(b0[1], b0[0] + args.compare_systems)
-    results, outs = {}, {}
+    results = {}
     for s in ("mixed", "lu_f64"):
-        t, n = timed(s, b0[0], cmp_hi)
-        outs[s] = y.cpu().numpy()[b0[0]:cmp_hi]
-        results[s] = {"systems_per_s": (cmp_hi - b0[0]) / t, "substeps": n,
-                      "systems": cmp_hi - b0[0], "timed": f"systems 0..{cmp_hi - 1}",
-                      "flagged_systems": int((status[b0[0]:cmp_hi].cpu().numpy() != 0).sum())}
-    mixed_over_fp64 = results["mixed"]["systems_per_s"] / results["lu_f64"]["systems_per_s"]
+        t, n = timed(s, *b0, timeout_s=args.compare_seconds)
+        results[s] = {"substeps_per_s": n / t,
+                      "timed": f"slice 0 under a {args.compare_seconds:g} s device deadline"}
+    mixed_over_fp64 = results["mixed"]["substeps_per_s"] / results["lu_f64"]["substeps_per_s"]
     main_solver = args.solver if args.solver != "auto" else max(
-        cand, key=lambda s: results[s]["systems_per_s"])
+        cand, key=lambda s: results[s]["substeps_per_s"])
 
     # ---- the timed job: every system once, K launches
     if dist is not None:
@@ -362,17 +371,20 @@ def run_main(args, wl, desc):
     steps_main = nsteps.cpu().numpy()
     results[main_solver + "_full_job"] = {"systems_per_s": S / sum(times), "substeps": substeps,
                                           "systems": S, "timed": "all slices",
-                                          "flagged_systems": int((st_main != 0).sum())}
-    outs[main_solver] = y_main
+                                          "status": status_counts(st_main)}
+    outs = {main_solver: y_main}
+    per_sys = float(steps_main[b0[0]:b0[1]].mean())
+    for s in ("mixed", "lu_f64"):
+        results[s]["systems_per_s"] = results[s]["substeps_per_s"] / per_sys
+        results[s]["systems_per_s_definition"] = "substeps/s / mean substeps per system of the main run"
 
     # ---- GJE_F64 (the reference's Gauss-Jordan in FP64): rate under a deadline
     t, n = timed("gje_f64", *b0, timeout_s=args.gje_seconds)
-    per_sys = float(steps_main[b0[0]:b0[1]].mean())
     results["gje_f64"] = {"substeps_per_s": n / t, "systems_per_s": n / t / per_sys,
                           "substeps": n, "timed": (f"slice 0 under a {args.gje_seconds:g} s device "
                                                    "deadline; systems/s = substeps/s / mean "
                                                    "substeps per system of the main run")}
-    mixed_over_gje = results["mixed"]["systems_per_s"] / results["gje_f64"]["systems_per_s"]
+    mixed_over_gje = results["mixed"]["substeps_per_s"] / results["gje_f64"]["substeps_per_s"]
 
     # ---- e2e through the C ABI with pinned host buffers (first slices)
     e2e_slices = bounds[:min(len(bounds), args.e2e_slices)]
@@ -410,7 +422,7 @@ def run_main(args, wl, desc):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_tot = float(tt.item())
     e2e_sys = e2e_hi - e2e_lo
-    e2e_same = np.array_equal(h_y.numpy(), y_main[e2e_lo:e2e_hi])
+    e2e_same = np.array_equal(h_y.numpy(), y_main[e2e_lo:e2e_hi], equal_nan=True)
 
     # ---- roofline of the integrate kernel
     fps = flops_per_substep(wl, args.method)
@@ -448,9 +460,13 @@ def run_main(args, wl, desc):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         n_cpu = reference_sample_size(wl, args.method, args.ref_seconds, cores)
-        n_cpu = min(n_cpu, cmp_hi - b0[0])
+        n_cpu = min(n_cpu, b0[1] - b0[0])
         if n_cpu > 0:
             dt, y_ref = reference_run(wl, 0, n_cpu, args.method, cores)
+            for s in ("mixed", "lu_f64"):
+                if s not in outs:
+                    timed(s, 0, n_cpu)
+                    outs[s] = y.cpu().numpy()[:n_cpu]
             cpu = {"value": n_cpu / dt, "unit": "systems/s", "cores": cores, "kind": "reference",
                    "sample": (f"systems 0..{n_cpu - 1} of {S:,}, {dt:.1f} s; c_baseline FP64 "
                               "(-Dfloat=double) built from the reference sources")}
@@ -477,7 +493,8 @@ def run_main(args, wl, desc):
             "data": "synthetic",
             "config": dict(config_dict(args, wl, desc), solver=main_solver),
             "solvers": results, "mixed_over_fp64": mixed_over_fp64,
-            "mixed_over_fp64_definition": "MIXED / LU_F64 systems/s on the same first systems",
+            "mixed_over_fp64_definition": ("MIXED / LU_F64 substeps/s on slice 0 under the same "
+                                           "device deadline (same systems, full occupancy)"),
             "mixed_over_gje_f64": mixed_over_gje,
             "max_rel_err_vs_reference": errs or None,
             "e2e": {"value": world * e2e_sys / e2e_tot, "unit": "systems/s",
@@ -559,7 +576,7 @@ def run_mixed(args):
         res[solver] = {"systems_per_s": nsys / statistics.median(times),
                        "ms_per_step": 1e3 * statistics.median(times),
                        "substeps": int(sum(int(g.nsteps.sum()) for g in dg)),
-                       "flagged_systems": int(sum(int((g.status != 0).sum()) for g in dg))}
+                       "status": status_counts(np.concatenate([g.status.cpu().numpy() for g in dg]))}
     line = {"metric": METRIC, "workload": "mixed", "unit": "systems/s",
             "value": res[solvers[-1]]["systems_per_s"], "steps": args.steps, "warmup": args.warmup,
             "config": {"workload": (f"{nsys:,} systems, N in {{5,16,32,64,157}} at 40/25/20/10/5 %, "
@@ -617,9 +634,9 @@ def main():
     ap.add_argument("--spec-width", type=int, default=0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--gje-seconds", type=float, default=3.0)
-    ap.add_argument("--e2e-slices", type=int, default=3)
-    ap.add_argument("--compare-systems", type=int, default=16384,
-                    help="systems of slice 0 integrated by both MIXED and LU_F64 for their ratio")
+    ap.add_argument("--e2e-slices", type=int, default=1)
+    ap.add_argument("--compare-seconds", type=float, default=4.0,
+                    help="device deadline of the MIXED and LU_F64 rate runs on slice 0")
     ap.add_argument("--traffic-per-system", type=float, default=0.0,
                     help="DRAM bytes per system per launch from an ncu capture (roofline.traffic)")
     ap.add_argument("--profile", action="store_true",

@@ -178,10 +178,10 @@ def test_mixed_size_single_launch(cuda_device, solver):
 def test_cta_mixed_fallback_flag(cuda_device):
     """MIXED inverts N > 32 systems by Gauss-Jordan without pivoting.  Here
     (I - hJ)[0][0] of the first full step is exactly zero (no reaction
-    touches species 0 and h L[0][0] = 1), so the inverse cannot be formed:
-    the substep is redone with the partial-pivoting LU, the system carries
-    WIND_SYS_REFINE_FALLBACK, and its result is the FP64 LU path's.  Species
-    0 and 1 are coupled through L so the matrix stays nonsingular."""
+    touches species 0 and h L[0][0] = 1), so that inverse cannot be formed:
+    the substep is redone with the pivoted Gauss-Jordan inverse, the system
+    carries WIND_SYS_REFINE_FALLBACK, and its result is the FP64 LU path's.
+    Species 0 and 1 are coupled through L so the matrix stays nonsingular."""
     rng = np.random.default_rng(7)
     n, s, dt = 40, 4, 1e-3
     net = W.random_mass_action(rng, s, n - 1, 80, 1e-3, 1e-1)

@@ -660,6 +660,7 @@ __device__ __forceinline__ double cta_max_abs(const CtaCtx& c, double v, int& ph
 static __device__ __noinline__ void cta_gj_invert(const CtaCtx& c, float* A) {
     const int N = c.N, tid = c.tid, ld = c.ld;
     const int nch = (N + 3) >> 2;  // 4-wide chunks holding rows / columns < N
+    if (tid < N) c.act[tid] = tid;   // row i expresses unknown i (no pivoting)
     for (int k0 = 0; k0 < N; k0 += CTA_NB) {
         const int kb = min(CTA_NB, N - k0);
         const int pc0 = k0 >> 2, pc1 = (k0 + kb + 3) >> 2;  // chunks touching P
@@ -781,6 +782,56 @@ static __device__ __noinline__ void cta_gj_invert(const CtaCtx& c, float* A) {
     }
 }
 
+// Gauss-Jordan inversion of A in place with partial pivoting and no row
+// exchanges, for systems whose matrices the unpivoted elimination cannot
+// handle (mass-action Jacobians are not diagonally dominant: a reaction
+// A + B -> C + D puts +h k y_B in row B of column A).  Column k's pivot is
+// the largest |a_ik| over the rows not yet chosen, voted CTA-wide as in
+// cta_lu (warp reduce, packed 64-bit atomicMax, rotating slots); the chosen
+// row is copied to a broadcast buffer and every thread updates its own row
+// over all N columns.  Two barriers per column.  On return row i expresses
+// unknown c.act[i]: x_{act[i]} = sum_j M[i][j] b_{p_j} with p_j the row
+// chosen at step j.
+static __device__ __noinline__ void cta_gj_invert_pivoted(const CtaCtx& c, float* A) {
+    const int N = c.N, tid = c.tid, ld = c.ld;
+    float* bc = static_cast<float*>(c.cand);  // >= 1280 bytes: one row of up to 256 + 4 floats
+    float* myrow = A + (size_t)(tid < N ? tid : 0) * ld;
+    bool done = tid >= N;
+    if (tid < 3) c.best[tid] = 0ull;
+    __syncthreads();
+    for (int k = 0; k < N; k++) {
+        const uint32_t key = done ? 0u : mag_key(myrow[k]) + 1u;
+        const uint32_t wmax = __reduce_max_sync(0xffffffffu, key);
+        const int wl = __ffs(__ballot_sync(0xffffffffu, key == wmax)) - 1;
+        if ((tid & 31) == wl && wmax)
+            atomicMax(c.best + k % 3, ((unsigned long long)wmax << 32) | (unsigned)(0xffff - tid));
+        __syncthreads();
+        if (tid == 0) c.best[(k + 2) % 3] = 0ull;
+        const int pr = 0xffff - (int)(c.best[k % 3] & 0xffffu);
+        if (tid == pr) {
+            for (int t = 0; t < N; t += 4) st4(bc + t, *reinterpret_cast<const float(*)[4]>(myrow + t));
+            c.act[tid] = k;
+            done = true;
+        }
+        __syncthreads();
+        if (tid < N) {
+            const float r = nr_rcp(bc[k]);
+            const float alpha = (tid == pr) ? r - 1.0f : -myrow[k] * r;
+            for (int t = 0; t < N; t += 4) {
+                float a[4], w[4];
+                ld4(myrow + t, a);
+                ld4(bc + t, w);
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (t + q != k) a[q] = fmaf(alpha, w[q], a[q]);
+                st4(myrow + t, a);
+            }
+            myrow[k] = (tid == pr) ? r : alpha;
+        }
+    }
+    __syncthreads();
+}
+
 // Row j of M times the FP32 vector qb (shared memory), four accumulators.
 __device__ __forceinline__ double cta_apply_row(const float* mrow, const float* qb, int N) {
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
@@ -811,29 +862,32 @@ static __device__ __noinline__ int cta_refine(const CtaCtx& c, const float* A, d
     const int N = c.N, j = c.tid, ld = c.ld;
     const bool own = j < N;
     // FP32 broadcast vector in the residual slot (c.r starts 32N bytes into
-    // the 16-byte aligned vector block, so float4 reads of it are aligned)
+    // the 16-byte aligned vector block, so float4 reads of it are aligned).
+    // Row j of the inverse gives unknown act[j]: right-hand sides are
+    // scattered to qb[act[j]], results gathered through c.x[act[j]].
     float* qb = reinterpret_cast<float*>(c.r);
-    if (own) qb[j] = (float)c.f[j];
+    const int sj = own ? c.act[j] : 0;
+    if (own) qb[sj] = (float)c.f[j];
     __syncthreads();
-    double xj = own ? cta_apply_row(A + (size_t)j * ld, qb, N) : 0.0;
-    const double xmax = cta_max_abs(c, xj, phase);
+    double xt = own ? cta_apply_row(A + (size_t)j * ld, qb, N) : 0.0;  // x_{act[j]}
+    const double xmax = cta_max_abs(c, xt, phase);
     double dprev = 0.0;
     int outcome = CTA_REFINE_GAVE_UP;
     for (int it = 0; it < maxit; it++) {
-        if (own) c.x[j] = xj;
+        if (own) c.x[sj] = xt;
         __syncthreads();
-        const double r = own ? c.f[j] - fma(-h, cta_jx(c, j, c.x), xj) : 0.0;
-        if (own) qb[j] = (float)r;
+        const double r = own ? c.f[j] - fma(-h, cta_jx(c, j, c.x), c.x[j]) : 0.0;
+        if (own) qb[sj] = (float)r;
         __syncthreads();
         const double d = own ? cta_apply_row(A + (size_t)j * ld, qb, N) : 0.0;
-        xj += d;
+        xt += d;
         const double dmax = cta_max_abs(c, d, phase);
         const double rho = (it == 0) ? dmax / fmax(xmax, 1e-300) : dmax / fmax(dprev, 1e-300);
         if (dmax * rho <= 0x1p-33 * xmax || dmax == 0.0) { outcome = CTA_REFINE_OK; break; }
         if (rho > (it == 0 ? abort0 : 0.5)) break;
         dprev = dmax;
     }
-    if (own) c.x[j] = xj;
+    if (own) c.x[sj] = xt;
     __syncthreads();
     return outcome;
 }
@@ -1111,6 +1165,7 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
         // MIXED: f(y) cached while y is unchanged; the matrix area holds the
         // inverse for the next full step; rotating max-slot phase
         bool fy_ok = false, inv_ok = false;
+        double h_pivot = INFINITY;  // MIXED: fresh inverses at this step size and above pivot
         double fyl = 0.0;
         int phase = 0;
         while (!bad && tnow < tend) {
@@ -1130,9 +1185,32 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
                 // previous attempt's half-step inverse (same y, same size)
                 // for the full step, a fresh one for the first half step,
                 // reused for the second half step while it still contracts.
+                // Fresh inverses are unpivoted (blocked, fast) below the
+                // smallest step size at which an unpivoted one failed to
+                // refine for this system, pivoted (column vote) at and above
+                // it: the growth of the unpivoted elimination rises with h.
+                // A fresh pivoted inverse that does not refine either (I - hJ
+                // too ill-conditioned for FP32) leaves the substep to the FP32
+                // LU recovery.  Any recovery flags the system
+                // WIND_SYS_REFINE_FALLBACK.
                 const double hf = t1 - tnow, h1 = (t1 - tnow) * 0.5;
                 const double h2 = (CTRL == WIND_CTRL_DEVICE) ? fmin(t1 - (tnow + h1), h1) : h1;
                 float* A = static_cast<float*>(mat);
+                // a fresh inverse of this substep's own matrix, and its solve
+                auto fresh_solve = [&](double hh) {
+                    cta_build<float>(c, hh, A);
+                    if (hh < h_pivot) {
+                        cta_gj_invert(c, A);
+                        if (cta_refine(c, A, hh, 24, 1.0, phase) == CTA_REFINE_OK) return true;
+                        h_pivot = hh;
+                        cta_build<float>(c, hh, A);
+                    }
+                    st |= WIND_SYS_REFINE_FALLBACK;
+                    cta_gj_invert_pivoted(c, A);
+                    if (cta_refine(c, A, hh, 24, 1.0, phase) == CTA_REFINE_OK) return true;
+                    cta_mixed_pivoted_solve(c, hh, A);
+                    return false;
+                };
                 if (own) c.v[tid] = yl;
                 __syncthreads();
                 if (!fy_ok) {
@@ -1143,37 +1221,16 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
                     if (own) c.f[tid] = fyl;
                     __syncthreads();
                 }
-                if (!inv_ok) {
-                    cta_build<float>(c, hf, A);
-                    cta_gj_invert(c, A);
-                }
-                if (cta_refine(c, A, hf, 8, 0.5, phase) != CTA_REFINE_OK) {
-                    st |= WIND_SYS_REFINE_FALLBACK;
-                    cta_mixed_pivoted_solve(c, hf, A);
-                }
+                if (!inv_ok || cta_refine(c, A, hf, 8, 0.5, phase) != CTA_REFINE_OK) fresh_solve(hf);
                 y1l = own ? yl + hf * c.x[tid] : 0.0;
-                cta_build<float>(c, h1, A);
-                cta_gj_invert(c, A);
-                inv_ok = true;
-                if (cta_refine(c, A, h1, 24, 1.0, phase) != CTA_REFINE_OK) {
-                    st |= WIND_SYS_REFINE_FALLBACK;
-                    cta_mixed_pivoted_solve(c, h1, A);
-                    inv_ok = false;
-                }
+                inv_ok = fresh_solve(h1);  // the inverse stays for the next full step
                 const double vhl = own ? yl + h1 * c.x[tid] : 0.0;
                 if (own) c.v[tid] = vhl;
                 __syncthreads();
                 cta_rhs_fast(c);
-                int out = CTA_REFINE_GAVE_UP;
-                if (inv_ok) out = cta_refine(c, A, h2, 8, 0.0625, phase);
-                if (out != CTA_REFINE_OK) {
-                    cta_build<float>(c, h2, A);
-                    cta_gj_invert(c, A);
+                if (!inv_ok || cta_refine(c, A, h2, 8, 0.0625, phase) != CTA_REFINE_OK) {
+                    fresh_solve(h2);
                     inv_ok = false;
-                    if (cta_refine(c, A, h2, 24, 1.0, phase) != CTA_REFINE_OK) {
-                        st |= WIND_SYS_REFINE_FALLBACK;
-                        cta_mixed_pivoted_solve(c, h2, A);
-                    }
                 }
                 y2l = own ? vhl + h2 * c.x[tid] : 0.0;
             } else

@@ -27,8 +27,9 @@
 //          predicted error is below 2^-33 |x|.  A refinement that stalls is
 //          restarted with a fresh inverse of the substep's own matrix; if that
 //          one does not refine either (I - hJ too ill-conditioned for FP32),
-//          the substep is solved by the plain FP64 LU and the system is
-//          flagged WIND_SYS_REFINE_FALLBACK.
+//          the substep is solved by the plain FP64 LU, the system is flagged
+//          WIND_SYS_REFINE_FALLBACK, and its substeps of that size and larger
+//          go straight to the FP64 LU from then on.
 // The step sizes, substep sequence, error test and accept/reject decisions
 // are the reference controller's (cuda/common/kernel.cu:191-296 DEVICE,
 // cuda/c_baseline/common/common_gold.c:48-153 GOLD); only the linear solve
@@ -539,6 +540,33 @@ __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_r
         T a[NMAX];
         int mystep = -1, svstep = -1;
         bool inv_ok = false;      // MIXED: the save area inverts I - h' J(y), h' the next full step
+        // MIXED: substeps of this size and larger go straight to the FP64 LU
+        // (a fresh FP32 inverse failed to refine at this size: I - hJ is too
+        // ill-conditioned for FP32 factors, and grows more so with h)
+        double h_fp64 = INFINITY;
+        // A fresh solve of the substep's own matrix (scatter rows of the
+        // state in vb): FP32 inverse and FP64 refinement, or the FP64 LU.
+        auto mixed_fresh = [&](double hh, double ff, bool save) -> double {
+            double xx = 0.0;
+            if constexpr (SOLVER == WIND_SOLVER_MIXED) {
+                if (hh < h_fp64) {
+                    warp_load_matrix(c, hh, a);
+                    mystep = warp_gj_invert(c, a);
+                    if (warp_refine(c, a, mystep, hh, ff, xx, WARP_MIX_MAXIT2, 0.25) == REFINE_OK) {
+                        if (save) {
+                            warp_save_inverse(c, a);
+                            svstep = mystep;
+                            inv_ok = true;
+                        }
+                        return xx;
+                    }
+                    h_fp64 = hh;
+                }
+                st |= WIND_SYS_REFINE_FALLBACK;
+                xx = warp_fp64_fallback(c, hh, ff);
+            }
+            return xx;
+        };
         while (!bad_idx && tnow < tend) {
             if (attempts >= p.max_attempts) { st |= WIND_SYS_MAX_ATTEMPTS; break; }
             if (p.timeout_ns) {
@@ -564,32 +592,18 @@ __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_r
                 // full step: the previous attempt's half-step inverse is
                 // the inverse of this matrix (same state, same size) when y
                 // is unchanged; else a fresh one
-                if (inv_ok) {
+                if (hf < h_fp64 && inv_ok) {
                     warp_load_inverse(c, a);
                     mystep = svstep;
+                    if (warp_refine(c, a, mystep, hf, fy, x, WARP_MIX_MAXIT, 0.5) != REFINE_OK)
+                        x = mixed_fresh(hf, fy, false);
                 } else {
-                    warp_load_matrix(c, hf, a);
-                    mystep = warp_gj_invert(c, a);
-                }
-                if (warp_refine(c, a, mystep, hf, fy, x, WARP_MIX_MAXIT, 0.5) != REFINE_OK) {
-                    warp_load_matrix(c, hf, a);
-                    mystep = warp_gj_invert(c, a);
-                    if (warp_refine(c, a, mystep, hf, fy, x, WARP_MIX_MAXIT2, 1.0) != REFINE_OK) {
-                        st |= WIND_SYS_REFINE_FALLBACK;
-                        x = warp_fp64_fallback(c, hf, fy);
-                    }
+                    x = mixed_fresh(hf, fy, false);
                 }
                 y1 = y + hf * x;
                 // first half step: a fresh inverse, saved for the next attempt
-                warp_load_matrix(c, h1, a);
-                mystep = warp_gj_invert(c, a);
-                warp_save_inverse(c, a);
-                svstep = mystep;
-                inv_ok = true;
-                if (warp_refine(c, a, mystep, h1, fy, x, WARP_MIX_MAXIT2, 1.0) != REFINE_OK) {
-                    st |= WIND_SYS_REFINE_FALLBACK;
-                    x = warp_fp64_fallback(c, h1, fy);
-                }
+                inv_ok = false;
+                x = mixed_fresh(h1, fy, true);
                 vh = y + h1 * x;
             } else {
                 warp_load_matrix(c, hf, a);
@@ -609,15 +623,11 @@ __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_r
                 // the half-step inverse again, if it still contracts well at
                 // vh (small steps); else an inverse of this substep's own
                 // matrix (the scatter rows then hold J(vh), not J(y))
-                if (warp_refine(c, a, mystep, h2, f2, x, WARP_MIX_MAXIT, 0.0625) != REFINE_OK) {
+                if (!inv_ok || h2 >= h_fp64 ||
+                    warp_refine(c, a, mystep, h2, f2, x, WARP_MIX_MAXIT, 0.0625) != REFINE_OK) {
                     warp_jma_row(c);
                     jy_ok = false;
-                    warp_load_matrix(c, h2, a);
-                    mystep = warp_gj_invert(c, a);
-                    if (warp_refine(c, a, mystep, h2, f2, x, WARP_MIX_MAXIT2, 1.0) != REFINE_OK) {
-                        st |= WIND_SYS_REFINE_FALLBACK;
-                        x = warp_fp64_fallback(c, h2, f2);
-                    }
+                    x = mixed_fresh(h2, f2, false);
                 }
                 y2 = vh + h2 * x;
             } else {
