@@ -75,15 +75,23 @@ enum { WIND_CTRL_DEVICE = 0, WIND_CTRL_GOLD = 1 };
  *          transposed matrix-vector product, in FP64, same operation order
  *          (cuda/c_baseline/linear_algebra/gje_gold.c:5-144,
  *           cuda/linear_algebra/gauss_jordan_elimination.cu:15-212).
- * LU_F64:  partial-pivot LU solve in FP64.
- * MIXED:   FP32 LU factors, FP64 residual from the network, FP64 iterative
- *          refinement.  N <= 32: partial pivoting.  32 < N: no pivoting
- *          (the reference's elimination order); a substep whose refinement
- *          does not converge (after two steps, a correction above 1e-6 of
- *          the largest |x| in its 32-row slice i, i+32, ...) is redone with
- *          partial pivoting and the system is flagged
- *          WIND_SYS_REFINE_FALLBACK. */
-enum { WIND_SOLVER_GJE_F64 = 0, WIND_SOLVER_LU_F64 = 1, WIND_SOLVER_MIXED = 2 };
+ * LU_F64:  partial-pivot LU solve in FP64 (the plain FP64 path).
+ * MIXED:   an FP32 Gauss-Jordan inverse of I - hJ computed once per
+ *          step-doubling attempt (at the half-step size) and reused as the
+ *          approximate inverse of the attempt's substeps -- and of the next
+ *          attempt's full step after a rejection -- inside an FP64 iterative
+ *          refinement r = f - (x - h J x), x += M r, with J x evaluated in FP64
+ *          from the network; stops when the predicted error is below 2^-33
+ *          max|x|.  N <= 32: the inverse is pivoted; a substep FP32 cannot
+ *          refine is solved by the FP64 LU.  32 < N: the inverse is unpivoted
+ *          and blocked, pivoted at and above the step size where the
+ *          unpivoted one failed to refine, and an FP32 LU recovery stands
+ *          behind both.  Any recovery flags the system
+ *          WIND_SYS_REFINE_FALLBACK.
+ * AUTO:    per network shape, the faster of the two measured on B200: LU_F64
+ *          for the compiled networks and N <= 32, MIXED above 32 species (one
+ *          persistent launch still serves a mixed-size batch). */
+enum { WIND_SOLVER_GJE_F64 = 0, WIND_SOLVER_LU_F64 = 1, WIND_SOLVER_MIXED = 2, WIND_SOLVER_AUTO = 3 };
 
 /* Network kinds: the ode_system plug-ins (cuda/include/device.h:1-13,
  * cuda/include/ode_gold.h:1-12).

@@ -43,7 +43,9 @@ MEM_DEVICE = 1
 
 METHODS = {"sie": METHOD_SIE, "rk2": METHOD_RK2}
 CONTROLLERS = {"device": CTRL_DEVICE, "gold": CTRL_GOLD}
-SOLVERS = {"gje_f64": SOLVER_GJE_F64, "lu_f64": SOLVER_LU_F64, "mixed": SOLVER_MIXED}
+SOLVER_AUTO = 3
+SOLVERS = {"gje_f64": SOLVER_GJE_F64, "lu_f64": SOLVER_LU_F64, "mixed": SOLVER_MIXED,
+           "auto": SOLVER_AUTO}
 
 
 class WindNetwork(C.Structure):

@@ -73,9 +73,11 @@ wind_status check_network(const wind_network* net, int64_t nsys) {
 
 // Launch the right kernel family for one homogeneous batch already on the
 // device.  `p.counters` must point at zeroed device counters.
-wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream_t stream,
+wind_status launch_integrate(const wind_options& o_in, const KParams& p, cudaStream_t stream,
                              bool allow_alloc) {
     if (p.nsys == 0) return WIND_OK;
+    wind_options o = o_in;
+    o.solver = resolve_solver(o.solver, p.kind, p.n_eq);
     if (p.kind != WIND_NET_MASS_ACTION) return launch_lane(o, p, stream);
     if (p.n_eq <= WIND_TEAM_MAX_EQ) return launch_team(o, p, stream);
     // CTA kernels: global scratch for the matrices that do not fit in shared

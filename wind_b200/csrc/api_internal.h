@@ -18,9 +18,16 @@ wind_status check_network(const wind_network* net, int64_t nsys);
 inline wind_status check_options(const wind_options& o) {
     if (o.method != WIND_METHOD_SIE && o.method != WIND_METHOD_RK2) return WIND_ERR_ARGUMENT;
     if (o.controller != WIND_CTRL_DEVICE && o.controller != WIND_CTRL_GOLD) return WIND_ERR_ARGUMENT;
-    if (o.solver < WIND_SOLVER_GJE_F64 || o.solver > WIND_SOLVER_MIXED) return WIND_ERR_ARGUMENT;
+    if (o.solver < WIND_SOLVER_GJE_F64 || o.solver > WIND_SOLVER_AUTO) return WIND_ERR_ARGUMENT;
     if (o.spec_width < 0 || o.max_attempts < 0 || !(o.timeout_s >= 0.0)) return WIND_ERR_ARGUMENT;
     return WIND_OK;
+}
+
+// The solver WIND_SOLVER_AUTO stands for on one network shape: the FP64 LU
+// for the compiled networks and up to 32 species, the mixed solve above.
+inline int resolve_solver(int solver, int kind, int n_eq) {
+    if (solver != WIND_SOLVER_AUTO) return solver;
+    return (kind == WIND_NET_MASS_ACTION && n_eq > 32) ? WIND_SOLVER_MIXED : WIND_SOLVER_LU_F64;
 }
 // Launch the kernel family for one homogeneous batch.  `allow_alloc` = false
 // makes configurations that need global scratch return WIND_ERR_UNSUPPORTED

@@ -19,6 +19,7 @@ static MixedFn mixed_by_solver(int solver) {
         switch (solver) {
         case WIND_SOLVER_GJE_F64: return k_mixed<METHOD, CTRL, WIND_SOLVER_GJE_F64>;
         case WIND_SOLVER_LU_F64: return k_mixed<METHOD, CTRL, WIND_SOLVER_LU_F64>;
+        case WIND_SOLVER_AUTO: return k_mixed<METHOD, CTRL, WIND_SOLVER_MIXED, WIND_SOLVER_LU_F64>;
         default: return k_mixed<METHOD, CTRL, WIND_SOLVER_MIXED>;
         }
     }
@@ -45,15 +46,17 @@ wind_status launch_mixed(const wind_options& o, const std::vector<KParams>& ps, 
     cap -= 1024;
     size_t smem = 0, gslot = 0;
     for (const KParams& p : ps) {
+        // the solver each group runs (AUTO: MIXED above 32 species, LU_F64 below)
+        const int gs = resolve_solver(solver, p.kind, p.n_eq);
         if (p.n_eq > 32) {
-            const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, solver, cap);
+            const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, gs, cap);
             smem = std::max(smem, (size_t)lay.bytes);
             gslot = std::max(gslot, lay.g_doubles);
         } else {
             const int nm = nmax_of(p.n_eq);
-            const bool reg = o.method == WIND_METHOD_SIE && solver != WIND_SOLVER_GJE_F64;
-            const size_t team_bytes = reg ? (size_t)WarpLayout(nm, p.n_react, p.linear != nullptr, solver).bytes
-                                          : (size_t)TeamLayout(nm, p.n_react, p.linear != nullptr, solver).bytes;
+            const bool reg = o.method == WIND_METHOD_SIE && gs != WIND_SOLVER_GJE_F64;
+            const size_t team_bytes = reg ? (size_t)WarpLayout(nm, p.n_react, p.linear != nullptr, gs).bytes
+                                          : (size_t)TeamLayout(nm, p.n_react, p.linear != nullptr, gs).bytes;
             smem = std::max(smem, (size_t)(MIXED_THREADS / nm) * team_bytes);
         }
     }

@@ -93,7 +93,7 @@ extern "C" int wind_integrate_global(const wind_options* opt_in, const wind_netw
     if (t_reached) *t_reached = tnow;
     if (nsys == 0) return WIND_OK;
     cudaStream_t stream = (cudaStream_t)stream_v;
-    GlobalFn fn = global_fn(net->kind, o.solver);
+    GlobalFn fn = global_fn(net->kind, resolve_solver(o.solver, net->kind, net->n_eq));
 
     IntegrateCall call;
     st = call.prepare(o, *net, tnow, tend, n_integration_steps, y, nsys, atol, rtol, nullptr, nullptr,

@@ -59,6 +59,7 @@ int cudaIntegrateSIE(float tnow, float tend, int n_integration_steps, float* con
     if (const char* s = std::getenv("WIND_LEGACY_SOLVER")) {
         if (!std::strcmp(s, "lu_f64")) o.solver = WIND_SOLVER_LU_F64;
         else if (!std::strcmp(s, "mixed")) o.solver = WIND_SOLVER_MIXED;
+        else if (!std::strcmp(s, "auto")) o.solver = WIND_SOLVER_AUTO;
     }
     int64_t total = 0;
     const int st = wind_integrate_global(&o, &net, (double)tnow, (double)tend, n_integration_steps,
@@ -90,6 +91,7 @@ int cudaIntegrateSystem(float tnow, float tend, int n_integration_steps, float* 
     if (const char* s = std::getenv("WIND_LEGACY_SOLVER")) {
         if (!std::strcmp(s, "lu_f64")) o.solver = WIND_SOLVER_LU_F64;
         else if (!std::strcmp(s, "mixed")) o.solver = WIND_SOLVER_MIXED;
+        else if (!std::strcmp(s, "auto")) o.solver = WIND_SOLVER_AUTO;
     }
     if (const char* s = std::getenv("WIND_LEGACY_CONTROLLER"))
         if (!std::strcmp(s, "gold")) o.controller = WIND_CTRL_GOLD;

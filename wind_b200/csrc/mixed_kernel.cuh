@@ -22,7 +22,9 @@ constexpr int MIXED_THREADS = CTA_THREADS;
 // Two blocks per SM (128 registers) for the LU and mixed solvers, whose team
 // and CTA paths fit that budget; the reference Gauss-Jordan keeps a row of M
 // and of the inverse per lane in registers and gets the whole file.
-template <int METHOD, int CTRL, int SOLVER>
+// SMALL is the solver of the groups with N <= 32 (SOLVER for the others);
+// the AUTO solver runs MIXED above 32 species and LU_F64 below in one launch.
+template <int METHOD, int CTRL, int SOLVER, int SMALL = SOLVER>
 __global__ void __launch_bounds__(MIXED_THREADS, SOLVER == WIND_SOLVER_GJE_F64 ? 1 : 2)
     k_mixed(const KParams* __restrict__ groups, const int* __restrict__ order, int ngroups,
             double* gscratch, size_t gstride, int smem_cap) {
@@ -30,12 +32,12 @@ __global__ void __launch_bounds__(MIXED_THREADS, SOLVER == WIND_SOLVER_GJE_F64 ?
     for (int gi = 0; gi < ngroups; gi++) {
         const KParams p = groups[order[gi]];
         if (p.nsys > 0) {
-            constexpr bool REG = METHOD == WIND_METHOD_SIE && SOLVER != WIND_SOLVER_GJE_F64;
+            constexpr bool REG = METHOD == WIND_METHOD_SIE && SMALL != WIND_SOLVER_GJE_F64;
             if (p.n_eq > 32) cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, gstride, smem_cap);
             else if constexpr (REG) {
-                if (p.n_eq > 16) warp_run<32, CTRL, SOLVER>(p, smem_raw);
-                else if (p.n_eq > 8) warp_run<16, CTRL, SOLVER>(p, smem_raw);
-                else warp_run<8, CTRL, SOLVER>(p, smem_raw);
+                if (p.n_eq > 16) warp_run<32, CTRL, SMALL>(p, smem_raw);
+                else if (p.n_eq > 8) warp_run<16, CTRL, SMALL>(p, smem_raw);
+                else warp_run<8, CTRL, SMALL>(p, smem_raw);
             } else {
                 if (p.n_eq > 16) team_run<32, METHOD, CTRL, SOLVER>(p, smem_raw);
                 else if (p.n_eq > 8) team_run<16, METHOD, CTRL, SOLVER>(p, smem_raw);

@@ -147,7 +147,9 @@ extern "C" int wind_integrate_batch_noalloc(const wind_options* opt_in, const wi
         // group has been cleared or launched
         if (p.nsys > 0 && p.kind == WIND_NET_MASS_ACTION && p.n_eq > wind::WIND_TEAM_MAX_EQ) {
             wind::CtaPlan pl;
-            const wind_status pst = wind::plan_cta(o, p, /*allow_global=*/false, &pl);
+            wind_options oc = o;
+            oc.solver = wind::resolve_solver(o.solver, p.kind, p.n_eq);
+            const wind_status pst = wind::plan_cta(oc, p, /*allow_global=*/false, &pl);
             if (pst != WIND_OK) return pst;
         }
     }

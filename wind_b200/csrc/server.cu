@@ -92,7 +92,8 @@ static size_t footprint(const ServerRequest& r, const wind_server_config& cfg) {
     size_t b = r.nsys * (size_t)r.N * 8 + r.constants.size() * 8 + r.rates.size() * 8 +
                r.species.size() * 2 + r.linear.size() * 4 + r.nsys * 12 + 64 * 8;
     if (r.kind == WIND_NET_MASS_ACTION && r.N > wind::WIND_TEAM_MAX_EQ) {
-        const int solver = (cfg.method == WIND_METHOD_RK2) ? WIND_SOLVER_LU_F64 : cfg.solver;
+        const int solver = (cfg.method == WIND_METHOD_RK2) ? WIND_SOLVER_LU_F64
+                                                             : wind::resolve_solver(cfg.solver, r.kind, r.N);
         b += wind::cta_scratch_bytes_per_block(r.N, r.n_react, !r.linear.empty(), solver) *
              (size_t)wind::device_sm_count() * 2;
     }
