@@ -10,8 +10,8 @@ reference arm's own semantics).
 
 The whole job -- all 262,144 systems over the full interval -- is timed once:
 the K timed steps are K launches over disjoint contiguous slices that
-together cover every system exactly once.  W warm-up steps run slices before
-the timed region (untimed).
+together cover every system exactly once, each on its own stream.  W warm-up
+launches on the first systems precede the timed region (untimed).
 
 * ``value``        systems/s of the MIXED solver (FP32 factors + FP64
                    refinement) with inputs resident in HBM, CUDA events around
@@ -32,8 +32,9 @@ the timed region (untimed).
 the mixed-size batch), ``mixed`` (the mixed-size batch in one launch) and
 ``serve`` (Poisson request streams) select the other workloads.
 ``--impl reference`` times only the reference's CPU integrator.
-``--gpus N`` (under torchrun) runs N independent replicas ("replicas only":
-systems are independent, there is no exchange step).
+``--gpus N`` (under torchrun) splits the same job into N contiguous shards,
+one per GPU (strong scaling; systems are independent, there is no exchange
+step), timed as the max over ranks.
 """
 from __future__ import annotations
 
@@ -57,14 +58,24 @@ METRIC = "systems/s at 1e-5 rel err vs FP64 (mixed vs plain FP64 GPU); serve p50
 
 
 # ---------------------------------------------------------------------------
-def make_workload(name: str, systems: int = 0, dt: float = 0.0):
+def make_workload(name: str, systems: int = 0, dt: float = 0.0, rank: int = 0, world: int = 1):
+    """The workload and its description; with world > 1 this rank's
+    contiguous shard of it (the job's size is fixed: strong scaling)."""
+    from wind_b200.replicas import shard_range
     if name == "dense":
         n = systems or 262144
-        wl = W.workload_dense(n)
+        b, e = shard_range(n, rank, world)
+        wl = W.workload_dense(e - b, first=b)
         t = dt or 1.0
         wl = W.Workload(wl.net, wl.y0, 0.0, t, wl.atol, wl.rtol, 1, 1, "dense32")
         return wl, (f"dense N=32 + 64 reactions, {n:,} systems (seed 2), dt={t:g}, "
                     "atol=1e-8 rtol=1e-6")
+    wl, desc = _make_other(name, systems, dt)
+    b, e = shard_range(wl.net.nsys, rank, world)
+    return (wl if world == 1 else wl.subset(slice(b, e))), desc
+
+
+def _make_other(name: str, systems: int, dt: float):
     if name == "katz96":
         n = systems or 65536
         wl = W.workload_katz96(n, atol=1e-8, rtol=1e-6)
@@ -243,13 +254,13 @@ def run_reference_arm(args, wl, desc):
               f"one contiguous shard per thread")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "systems/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config_dict(args, wl, desc),
             "cpu_baseline": {"value": value, "unit": "systems/s", "cores": cores,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "systems/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(finite_json(line)), flush=True)
 
 
 STATUS_BITS = {1: "nonfinite", 2: "max_attempts", 4: "stalled", 8: "refine_fallback",
@@ -263,6 +274,29 @@ def status_counts(st) -> dict:
             if ((st & bit) != 0).any()}
 
 
+def error_stats(y, y_ref, atol: float) -> dict:
+    """Max relative error of y against y_ref ([S, N]) over the systems finite
+    in both, and how many systems diverge in both or in only one of them."""
+    fa = np.isfinite(y).all(axis=1)
+    fr = np.isfinite(y_ref).all(axis=1)
+    both = fa & fr
+    e = (np.abs(y[both] - y_ref[both]) / np.maximum(np.abs(y_ref[both]), atol)) if both.any() else None
+    return {"max_rel_err": float(e.max()) if e is not None else None,
+            "finite_systems": int(both.sum()), "nonfinite_both": int((~fa & ~fr).sum()),
+            "finiteness_differs": int((fa != fr).sum())}
+
+
+def finite_json(obj):
+    """obj with every non-finite float replaced by None (strict JSON)."""
+    if isinstance(obj, float):
+        return obj if np.isfinite(obj) else None
+    if isinstance(obj, dict):
+        return {k: finite_json(v) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return [finite_json(v) for v in obj]
+    return obj
+
+
 def config_dict(args, wl, desc):
     return {"workload": desc, "method": args.method, "controller": args.controller,
             "systems": wl.net.nsys, "equations": wl.net.n_eq,
@@ -270,8 +304,9 @@ def config_dict(args, wl, desc):
                    "read (the dense workload's 1.4 GB of inputs exceed L2); L2 flushed by a 256 MB "
                    "write before the timed region and before each solver-rate run"),
             "steps_cover": ("the K timed steps are K launches over disjoint slices covering every "
-                            "system once, alternating between two streams"),
-            "parallelism": f"replicas x{int(os.environ.get('WORLD_SIZE', '1'))}"}
+                            "system once, each on its own stream"),
+            "parallelism": (f"{int(os.environ.get('WORLD_SIZE', '1'))} independent shards of the "
+                            "job, one per GPU (no exchange step)")}
 
 
 # ---------------------------------------------------------------------------
@@ -348,30 +383,29 @@ def run_main(args, wl, desc):
     main_solver = args.solver if args.solver != "auto" else max(
         cand, key=lambda s: results[s]["substeps_per_s"])
 
-    # ---- the timed job: every system once, K launches.  The launches
-    # alternate between two streams, so the tail of one slice (its longest
-    # systems) overlaps the start of the next, as the tail of one launch over
-    # all systems would be a single one; each input byte is read once (the
-    # job's inputs are larger than L2), and the region spans the first launch
-    # to the last completion.
-    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
+    # ---- the timed job: every system once, K launches, each on its own
+    # stream.  A persistent launch frees its SMs block by block as its queue
+    # drains, so the next slice's blocks start beside the previous slice's
+    # longest systems (the ones the refinement cap holds for ~10^6 substeps)
+    # instead of waiting behind them, as in one launch over all systems; each
+    # input byte is read once (the job's inputs are larger than L2), and the
+    # region spans the first launch to the last completion.
+    streams = [torch.cuda.Stream(dev) for _ in bounds]
     y.copy_(y0)
     flush.zero_()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize(dev)
     launches0 = lib.launch_count()
-    counts = []
     o_main = lib.options(args.method, main_solver, args.controller, args.spec_width)
     with ClockSampler(local) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(streams[0])
-        streams[1].wait_event(e0)
+        e0.record(stream)
         done = []
         for i, (s0, s1) in enumerate(bounds):
-            ss = streams[i % 2]
+            ss = streams[i]
+            ss.wait_event(e0)
             ns = _capi.network_struct(net, {k: v[s0:s1] for k, v in d_arr.items()})
-            total = C.c_int64(0)
             code = wlib.wind_integrate(C.byref(o_main), C.byref(ns), wl.tnow, wl.tend,
                                        wl.n_integration_steps, y[s0:s1].data_ptr(), s1 - s0, wl.atol,
                                        wl.rtol, status[s0:s1].data_ptr(), nsteps[s0:s1].data_ptr(),
@@ -381,10 +415,9 @@ def run_main(args, wl, desc):
             ev = torch.cuda.Event()
             ev.record(ss)
             done.append(ev)
-        streams[0].wait_event(done[-1])
-        if len(done) > 1:
-            streams[0].wait_event(done[-2])
-        e1.record(streams[0])
+        for ev in done:
+            stream.wait_event(ev)
+        e1.record(stream)
         torch.cuda.synchronize(dev)
     if dist is not None:
         dist.barrier()
@@ -397,12 +430,17 @@ def run_main(args, wl, desc):
         tt = torch.tensor([tot], dtype=torch.float64, device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         tot = float(tt.item())
-    value = world * S / tot
+    s_job = S
+    if dist is not None:
+        tt = torch.tensor([S], dtype=torch.int64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.SUM)
+        s_job = int(tt.item())
+    value = s_job / tot
     y_main = y.cpu().numpy()
     st_main = status.cpu().numpy()
     steps_main = nsteps.cpu().numpy()
     results[main_solver + "_full_job"] = {"systems_per_s": S / tot, "substeps": substeps,
-                                          "systems": S, "timed": "all slices, two streams",
+                                          "systems": S, "timed": "all slices, one stream each",
                                           "status": status_counts(st_main)}
     outs = {main_solver: y_main}
     per_sys = float(steps_main[b0[0]:b0[1]].mean())
@@ -418,42 +456,65 @@ def run_main(args, wl, desc):
                                                    "substeps per system of the main run")}
     mixed_over_gje = results["mixed"]["substeps_per_s"] / results["gje_f64"]["substeps_per_s"]
 
-    # ---- e2e through the C ABI with pinned host buffers (first slices)
-    e2e_slices = bounds[:min(len(bounds), args.e2e_slices)]
-    e2e_lo, e2e_hi = e2e_slices[0][0], e2e_slices[-1][1]
+    # ---- e2e through the C ABI with pinned host buffers: the first
+    # --e2e-systems systems as --e2e-calls concurrent wind_integrate calls
+    # (host memory mode: each uploads its inputs, integrates and downloads
+    # its state on its own stream, from its own host thread -- ctypes
+    # releases the GIL), so one call's slowest systems overlap the others'
+    # work as in the resident run.  Device time: an event before every
+    # call's upload to an event after every call's download.
+    e2e_lo, e2e_hi = 0, min(S, args.e2e_systems)
+    e2e_calls = [(int(a0), int(a1)) for a0, a1 in zip(
+        np.linspace(e2e_lo, e2e_hi, args.e2e_calls + 1).round()[:-1],
+        np.linspace(e2e_lo, e2e_hi, args.e2e_calls + 1).round()[1:]) if a1 > a0]
     h_arr = {k: torch.from_numpy(np.ascontiguousarray(getattr(net, k)[e2e_lo:e2e_hi])).pin_memory()
              for k in keys}
     h_y0 = torch.from_numpy(np.ascontiguousarray(wl.y0[e2e_lo:e2e_hi])).pin_memory()
-    h_y = torch.empty_like(h_y0).pin_memory()
+    h_y = h_y0.clone().pin_memory()
     o = lib.options(args.method, main_solver, args.controller, args.spec_width)
-    e2e_times, h2d, d2h = [], 0, 0
-    for (s0, s1) in e2e_slices:
-        a0, a1 = s0 - e2e_lo, s1 - e2e_lo
-        h_y[a0:a1].copy_(h_y0[a0:a1])
-        sub = {k: v[a0:a1] for k, v in h_arr.items()}
-        hns = _capi.network_struct(net, sub)
-        flush.zero_()
-        torch.cuda.synchronize(dev)
-        total = C.c_int64(0)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        code = wlib.wind_integrate(C.byref(o), C.byref(hns), wl.tnow, wl.tend,
-                                   wl.n_integration_steps, h_y[a0:a1].data_ptr(), s1 - s0, wl.atol,
-                                   wl.rtol, None, None, C.byref(total), _capi.MEM_HOST,
-                                   stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        if code != 0:
-            raise RuntimeError(f"e2e wind_integrate failed: {code}")
-        e2e_times.append(e0.elapsed_time(e1) * 1e-3)
-        h2d += (s1 - s0) * N * 8 + sum(v[a0:a1].numel() * v.element_size() for v in h_arr.values())
-        d2h += (s1 - s0) * N * 8 + 8
+    e2e_streams = [torch.cuda.Stream(dev) for _ in e2e_calls]
+    codes = [None] * len(e2e_calls)
+
+    def e2e_call(i):
+        a0, a1 = e2e_calls[i]
+        torch.cuda.set_device(dev)
+        hns = _capi.network_struct(net, {k: v[a0:a1] for k, v in h_arr.items()})
+        codes[i] = wlib.wind_integrate(C.byref(o), C.byref(hns), wl.tnow, wl.tend,
+                                       wl.n_integration_steps, h_y[a0:a1].data_ptr(), a1 - a0,
+                                       wl.atol, wl.rtol, None, None, None, _capi.MEM_HOST,
+                                       e2e_streams[i].cuda_stream)
+
+    flush.zero_()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for ss in e2e_streams:
+        ss.wait_event(e0)
+    threads = [threading.Thread(target=e2e_call, args=(i,)) for i in range(len(e2e_calls))]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    for ss in e2e_streams:
+        stream.wait_stream(ss)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if any(c != 0 for c in codes):
+        raise RuntimeError(f"e2e wind_integrate failed: {codes}")
+    e2e_times = [e0.elapsed_time(e1) * 1e-3]
+    h2d = (e2e_hi - e2e_lo) * N * 8 + sum(v.numel() * v.element_size() for v in h_arr.values())
+    d2h = (e2e_hi - e2e_lo) * N * 8 + 8 * len(e2e_calls)
     e2e_tot = sum(e2e_times)
     if dist is not None:
         tt = torch.tensor([e2e_tot], dtype=torch.float64, device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_tot = float(tt.item())
     e2e_sys = e2e_hi - e2e_lo
+    e2e_job = e2e_sys
+    if dist is not None:
+        tt = torch.tensor([e2e_sys], dtype=torch.int64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.SUM)
+        e2e_job = int(tt.item())
     e2e_same = np.array_equal(h_y.numpy(), y_main[e2e_lo:e2e_hi], equal_nan=True)
 
     # ---- roofline of the integrate kernel
@@ -469,9 +530,12 @@ def run_main(args, wl, desc):
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     # DRAM bytes per launch from an ncu capture of the same kernel on a
     # smaller batch, scaled by systems (every system's network and state cross
-    # HBM once per launch, so traffic grows in proportion to the systems)
-    traffic_per_system = {("dense", "mixed"): args.traffic_per_system,
-                          ("katz96", "lu_f64"): 136.7}.get((args.workload, main_solver), 0.0)
+    # HBM once per launch, so traffic grows in proportion to the systems):
+    # k_warp LU_F64 on 4,096 dense systems read 22.2 MB (5,420 B per system
+    # against 5,376 B of network and state; its state writes were still in L2
+    # when the capture ended), k_lane LU_F64 on 16,384 Katz96 cells 136.7 B
+    traffic_per_system = args.traffic_per_system or {
+        ("dense", "lu_f64"): 5420.0, ("katz96", "lu_f64"): 136.7}.get((args.workload, main_solver), 0.0)
     traffic = traffic_per_system * S / len(bounds) if traffic_per_system else None
     roof = {"bound": "fp32" if fp32_main else "fp64", "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
@@ -503,10 +567,10 @@ def run_main(args, wl, desc):
                    "sample": (f"systems 0..{n_cpu - 1} of {S:,}, {dt:.1f} s; c_baseline FP64 "
                               "(-Dfloat=double) built from the reference sources")}
             for s, yy in outs.items():
-                a = yy[:n_cpu]
-                errs[s] = float(np.max(np.abs(a - y_ref) / np.maximum(np.abs(y_ref), wl.atol)))
+                errs[s] = error_stats(yy[:n_cpu], y_ref, wl.atol)
             errs["systems"] = n_cpu
-            errs["metric"] = "max |y - y_ref| / max(|y_ref|, atol)"
+            errs["metric"] = ("max |y - y_ref| / max(|y_ref|, atol) over the systems finite in "
+                              "both; systems that diverge (non-finite) are counted")
 
     # ---- config 2 (Katz96) beside the headline, cheap
     extra = None
@@ -520,7 +584,7 @@ def run_main(args, wl, desc):
         return
     line = {"metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(bounds),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32 factors + f64 refinement, f64 state" if fp32_main else "f64",
             "data": "synthetic",
             "config": dict(config_dict(args, wl, desc), solver=main_solver),
@@ -529,14 +593,15 @@ def run_main(args, wl, desc):
                                            "device deadline (same systems, full occupancy)"),
             "mixed_over_gje_f64": mixed_over_gje,
             "max_rel_err_vs_reference": errs or None,
-            "e2e": {"value": world * e2e_sys / e2e_tot, "unit": "systems/s",
-                    "h2d_bytes_per_step": int(h2d / len(e2e_slices)),
-                    "d2h_bytes_per_step": int(d2h / len(e2e_slices)),
-                    "systems": e2e_sys, "slices": len(e2e_slices),
+            "e2e": {"value": e2e_job / e2e_tot, "unit": "systems/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "systems": e2e_sys, "calls": len(e2e_calls),
+                    "step": (f"systems 0..{e2e_sys - 1} as {len(e2e_calls)} concurrent "
+                             "wind_integrate calls on host buffers, one stream each"),
                     "state_equals_resident_run": bool(e2e_same)},
             "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk.summary(), "config2_katz96": extra}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(finite_json(line)), flush=True)
 
 
 def katz96_extra(args, torch, dev, lib, _capi, C):
@@ -641,7 +706,50 @@ def run_mixed(args):
             "mixed_over_fp64_definition": ("batch time with LU_F64 / with MIXED, each class's "
                                            "substeps at that solver's per-class rate under a "
                                            f"{args.compare_seconds:g} s device deadline")}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(finite_json(line)), flush=True)
+
+
+def run_ntile(args):
+    """Katz96 tiled Ntile times (the Precompiler's tiling; the reference's
+    NtileScaling sweep, python/ntbks/NtileScaling.ipynb, varies Ntile 1-50):
+    device time of one wind_integrate call per (Ntile, method, solver), on
+    resident inputs, median of --steps calls after --warmup."""
+    import torch
+    from wind_b200 import lib
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    cells = args.systems or 65536
+    base = W.workload_katz96(cells, atol=args.ntile_tol, rtol=args.ntile_tol)
+    rows = []
+    for nt in [int(x) for x in args.ntiles.split(",")]:
+        wl = W.tile_workload(base, nt)
+        d = {"constants": torch.from_numpy(wl.net.constants).to(dev)}
+        y0 = torch.from_numpy(wl.y0).to(dev)
+        for method, tend, solvers in (("sie", 1e13, ("gje_f64", "lu_f64")), ("rk2", 1e9, ("gje_f64",))):
+            for solver in solvers:
+                ts = []
+                for i in range(args.warmup + args.steps):
+                    y = y0.clone()
+                    torch.cuda.synchronize(dev)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    tot, st, _ = lib.integrate(wl.net, y, 0.0, tend, wl.atol, wl.rtol, method, solver,
+                                               args.controller, device_arrays=d)
+                    e1.record()
+                    torch.cuda.synchronize(dev)
+                    if i >= args.warmup:
+                        ts.append(e0.elapsed_time(e1))
+                rows.append({"ntile": nt, "neqn": 5 * nt, "method": method, "solver": solver,
+                             "interval_s": tend, "ms": statistics.median(ts), "substeps": tot,
+                             "flagged": int((st.cpu().numpy() != 0).sum())})
+    line = {"metric": "time per call vs equations per system (tiled Katz96)", "workload": "ntile",
+            "unit": "ms", "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": (f"Katz96 (seed 1), {cells:,} cells, each tiled Ntile times "
+                                    f"(identical tiles, shared constants), atol=rtol={args.ntile_tol:g}, "
+                                    "SIE over 1e13 s, RK2 over 1e9 s, one call"),
+                       "controller": args.controller},
+            "rows": rows}
+    print(json.dumps(finite_json(line)), flush=True)
 
 
 def run_serve(args):
@@ -668,7 +776,7 @@ def run_serve(args):
                                     "atol 1e-6 rtol 1e-4, seed 4+i"),
                        "max_inflight": 4},
             "rates": out}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(finite_json(line)), flush=True)
 
 
 def main():
@@ -687,7 +795,10 @@ def main():
     ap.add_argument("--spec-width", type=int, default=0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--gje-seconds", type=float, default=3.0)
-    ap.add_argument("--e2e-slices", type=int, default=1)
+    ap.add_argument("--e2e-systems", type=int, default=65536,
+                    help="systems of the end-to-end (host buffer) measurement")
+    ap.add_argument("--e2e-calls", type=int, default=8,
+                    help="concurrent wind_integrate calls the end-to-end systems are split into")
     ap.add_argument("--compare-seconds", type=float, default=4.0,
                     help="device deadline of the MIXED and LU_F64 rate runs on slice 0")
     ap.add_argument("--traffic-per-system", type=float, default=0.0,
@@ -699,6 +810,9 @@ def main():
                     help="device deadline per launch in seconds (bounds a profiled launch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--ntiles", default="1,2,5,10,20,50", help="Ntile values of --workload ntile")
+    ap.add_argument("--ntile-tol", type=float, default=5e-3,
+                    help="atol = rtol of --workload ntile (the reference sweep's 5e-3)")
     ap.add_argument("--rates", default="10,30,100,300,1000,2000", help="serving request rates (Hz)")
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--max-cells", type=int, default=2000)
@@ -711,9 +825,16 @@ def main():
         return run_serve(args)
     if args.workload == "mixed":
         return run_mixed(args)
-    wl, desc = make_workload(args.workload, args.systems, args.dt)
+    if args.workload == "ntile":
+        return run_ntile(args)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
+        if rank != 0:
+            return None
+        wl, desc = make_workload(args.workload, args.systems, args.dt)
         return run_reference_arm(args, wl, desc)
+    wl, desc = make_workload(args.workload, args.systems, args.dt, rank, world)
     if args.profile:
         return run_profile(args, wl, desc)
     return run_main(args, wl, desc)

@@ -53,6 +53,10 @@ build_net () {    # $1 = name, $2 = NUM_CONST, $3 = plugin source, $4 = extra de
 build_net katz96 10 "$REF/cuda/ode_system/ode_gold.c"
 build_net nr_test 4 "$HERE/plugins/nr_test_gold.c"
 build_net stifftrig 2 "$HERE/plugins/stifftrig_gold.c"
+# Katz96 tiled by the Precompiler's Ntile (one system of Ntile copies)
+for nt in 3 8; do
+    build_net "katz96_t$nt" 10 "$HERE/plugins/katz96_tiled_gold.c" "-DNTILE=$nt"
+done
 # Mass-action networks: ma_n<N>_r<R>[_lin]
 for spec in "5 50 0" "16 160 0" "32 320 0" "64 640 0" "157 1570 0" "32 64 1" \
             "3 6 1" "8 20 0" "12 30 1"; do

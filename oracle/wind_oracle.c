@@ -22,7 +22,7 @@
 
 #include "../include/wind.h"
 
-#define ORACLE_MAXN 160
+#define ORACLE_MAXN 320
 
 /* ------------------------------------------------------------------------ */
 /* ode_system plug-ins: RHS f and transposed Jacobian Jt[i*N+j] = df_j/dy_i  */
@@ -44,8 +44,7 @@ static void nr_jac(const double* c, double* J) {
 /* Katz96, cuda/ode_system/ode_gold.c:3-48 (RHS) and :50-93 (Jacobian),
  * same expression order.  J[13] = J[12] keeps the reference's sign
  * (ode_gold.c:79, device_dydt.cu:91): parity is with what it computes. */
-static void katz_rhs(const double* c, const double* y, double* f) {
-    double ne = y[1] + y[3] + y[4] * 2.0;
+static void katz_rhs_ne(const double* c, double ne, const double* y, double* f) {
     f[0] = c[2] * ne * y[1] - (c[0] * ne + c[1]) * y[0];
     f[1] = -c[2] * ne * y[1] + (c[0] * ne + c[1]) * y[0];
     f[2] = (c[7] + c[8]) * ne * y[3] - (c[3] * ne + c[4]) * y[2];
@@ -53,8 +52,7 @@ static void katz_rhs(const double* c, const double* y, double* f) {
          - (c[7] + c[8]) * ne * y[3] - (c[5] * ne + c[6]) * y[3];
     f[4] = (c[5] * ne + c[6]) * y[3] - c[9] * ne * y[4];
 }
-static void katz_jac(const double* c, const double* y, double* J) {
-    double ne = y[1] + y[3] + y[4] * 2.0;
+static void katz_jac_ne(const double* c, double ne, double* J) {
     J[0] = -(c[0] * ne + c[1]);
     J[1] = -J[0];
     J[6] = -c[2] * ne;
@@ -67,6 +65,9 @@ static void katz_jac(const double* c, const double* y, double* J) {
     J[24] = -c[9] * ne;
     J[23] = -J[24];
 }
+
+/* the generated prefix: ne from equations 1, 3, 4 (katz96.py:485-500) */
+static double katz_ne(const double* y) { return y[1] + y[3] + y[4] * 2.0; }
 
 /* StiffTrig, python/ode_systems/stifftrig.py:639-647 (RHS), :625-637 (J). */
 static void trig_rhs(const double* c, const double* y, double* f) {
@@ -132,13 +133,39 @@ typedef struct {
     int64_t s;
 } sysref;
 
+/* Equations per copy of a builtin network; n_eq = Ntile x base_n for the
+ * Precompiler's tiling (python/ode_systems/ode_base.py:86-88, 219-281): tile
+ * t owns equations [t*base_n, (t+1)*base_n), every tile uses the system's
+ * one set of constants, the Jacobian is block diagonal (reindex,
+ * ode_base.py:86-88), and Katz96's ne comes from tile 0 (the prefix is not
+ * reindexed, katz96.py:331-448). */
+static int base_n(int kind) { return kind == WIND_NET_KATZ96 ? 5 : 2; }
+
+static int net_ok(const wind_network* net) {
+    if (!net || net->n_eq < 1 || net->n_eq > ORACLE_MAXN) return 0;
+    if (net->kind == WIND_NET_MASS_ACTION) return 1;
+    if (net->kind != WIND_NET_NR_TEST && net->kind != WIND_NET_KATZ96 &&
+        net->kind != WIND_NET_STIFFTRIG)
+        return 0;
+    return net->n_eq % base_n(net->kind) == 0;
+}
+
 static void eval_rhs(const sysref* sr, const double* y, double* f) {
     const wind_network* n = sr->net;
     const double* c = n->constants ? n->constants + sr->s * n->n_const : NULL;
+    const int b = base_n(n->kind), nt = n->n_eq / b;
     switch (n->kind) {
-    case WIND_NET_NR_TEST: nr_rhs(c, y, f); break;
-    case WIND_NET_KATZ96: katz_rhs(c, y, f); break;
-    case WIND_NET_STIFFTRIG: trig_rhs(c, y, f); break;
+    case WIND_NET_NR_TEST:
+        for (int t = 0; t < nt; t++) nr_rhs(c, y + t * b, f + t * b);
+        break;
+    case WIND_NET_KATZ96: {
+        double ne = katz_ne(y);
+        for (int t = 0; t < nt; t++) katz_rhs_ne(c, ne, y + t * b, f + t * b);
+        break;
+    }
+    case WIND_NET_STIFFTRIG:
+        for (int t = 0; t < nt; t++) trig_rhs(c, y + t * b, f + t * b);
+        break;
     default: {
         int N = n->n_eq, R = n->n_react;
         ma_rhs(N, R, n->rates + sr->s * R, n->species + sr->s * R * 4,
@@ -153,10 +180,22 @@ static void eval_jac(const sysref* sr, const double* y, double* J) {
     int N = n->n_eq;
     memset(J, 0, sizeof(double) * N * N);
     const double* c = n->constants ? n->constants + sr->s * n->n_const : NULL;
+    if (n->kind != WIND_NET_MASS_ACTION) {
+        /* each tile's block written at its place on the diagonal */
+        const int b = base_n(n->kind), nt = N / b;
+        double ne = n->kind == WIND_NET_KATZ96 ? katz_ne(y) : 0.0;
+        for (int t = 0; t < nt; t++) {
+            double Jb[25];
+            memset(Jb, 0, sizeof(Jb));
+            if (n->kind == WIND_NET_NR_TEST) nr_jac(c, Jb);
+            else if (n->kind == WIND_NET_KATZ96) katz_jac_ne(c, ne, Jb);
+            else trig_jac(c, Jb);
+            for (int r = 0; r < b; r++)
+                for (int q = 0; q < b; q++) J[(t * b + r) * N + t * b + q] = Jb[r * b + q];
+        }
+        return;
+    }
     switch (n->kind) {
-    case WIND_NET_NR_TEST: nr_jac(c, J); break;
-    case WIND_NET_KATZ96: katz_jac(c, y, J); break;
-    case WIND_NET_STIFFTRIG: trig_jac(c, J); break;
     default: {
         int R = n->n_react;
         ma_jac(N, R, n->rates + sr->s * R, n->species + sr->s * R * 4,
@@ -331,7 +370,7 @@ int64_t wind_oracle_integrate(int method, int ctrl, const wind_network* net,
                               double* y, int64_t s_begin, int64_t s_end,
                               double atol, double rtol, int64_t max_attempts,
                               int32_t* status, int64_t* sys_nsteps) {
-    if (!net || !y || net->n_eq < 1 || net->n_eq > ORACLE_MAXN ||
+    if (!net_ok(net) || !y ||
         n_integration_steps < 1)
         return -1;
     if (max_attempts <= 0) max_attempts = (int64_t)1 << 40;
@@ -356,7 +395,7 @@ int64_t wind_oracle_integrate(int method, int ctrl, const wind_network* net,
 /* RHS and transposed Jacobian of one system, for plug-in tests. */
 int wind_oracle_rhs_jac(const wind_network* net, int64_t s, const double* y,
                         double* f, double* Jt) {
-    if (!net || net->n_eq < 1 || net->n_eq > ORACLE_MAXN) return -1;
+    if (!net_ok(net)) return -1;
     sysref sr = {net, s};
     if (f) eval_rhs(&sr, y, f);
     if (Jt) eval_jac(&sr, y, Jt);
@@ -366,7 +405,7 @@ int wind_oracle_rhs_jac(const wind_network* net, int64_t s, const double* y,
 /* One SIE substep of one system (tests of the solver paths). */
 int wind_oracle_sie_substep(const wind_network* net, int64_t s, int ctrl,
                             double h, double* y) {
-    if (!net || net->n_eq < 1 || net->n_eq > ORACLE_MAXN) return -1;
+    if (!net_ok(net)) return -1;
     scratch_t* w = (scratch_t*)malloc(sizeof(scratch_t));
     if (!w) return -1;
     sysref sr = {net, s};
@@ -390,7 +429,7 @@ int wind_oracle_sie_substep(const wind_network* net, int64_t s, int ctrl,
 int64_t wind_oracle_integrate_global(const wind_network* net, double tnow, double tend,
                                      int n_integration_steps, double* y, int64_t nsys,
                                      double atol, double rtol, double* t_reached) {
-    if (!net || !y || net->n_eq < 1 || net->n_eq > ORACLE_MAXN || n_integration_steps < 1 ||
+    if (!net_ok(net) || !y || n_integration_steps < 1 ||
         nsys < 0)
         return -1;
     int n = net->n_eq;

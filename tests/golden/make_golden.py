@@ -43,6 +43,9 @@ def reference_fixture(path=FIXTURE):
     return W.Workload(net, eq, 0.0, 10.0, float(np.float32(5e-3)), float(np.float32(5e-3)), 1, 1)
 
 
+Y_HE = W.Y_HELIUM
+
+
 def cases():
     out = []
     if REFERENCE and os.path.exists(FIXTURE):
@@ -56,6 +59,19 @@ def cases():
     out.append(("katz96_sie", "sie", k))
     out.append(("katz96_sie_tight", "sie", W.Workload(k.net, k.y0, 0.0, 1e11, 1e-8, 1e-6, 1, 1)))
     out.append(("katz96_rk2", "rk2", W.Workload(k.net, k.y0, 0.0, 1e6, 5e-3, 5e-3, 1, 1)))
+    # Ntile tiling (the reference's oracle build katz96_t<Ntile>): 3 tiles
+    # starting in different states, so the tiles differ and the shared
+    # electron density of tile 0 couples them; 8 identical tiles, as the
+    # reference's tileEquations makes them
+    kt = W.workload_katz96(8, seed=103)
+    y3 = np.tile(kt.y0, (1, 3))
+    y3[:, 5:10] = [0.3, 0.7, 0.02, Y_HE - 0.02, 0.0]
+    y3[:, 10:15] = [0.9, 0.1, Y_HE, 0.0, 0.0]
+    t3 = W.Workload(W.tile_network(kt.net, 3), y3, 0.0, 1e11, 1e-8, 1e-6, 1, 1)
+    out.append(("katz96_t3_sie", "sie", t3))
+    out.append(("katz96_t3_rk2", "rk2", W.Workload(t3.net, y3, 0.0, 1e6, 5e-3, 5e-3, 1, 1)))
+    out.append(("katz96_t8_sie", "sie",
+                W.tile_workload(W.Workload(kt.net, kt.y0, 0.0, 1e12, 1e-8, 1e-6, 1, 1), 8)))
     t = W.Workload(W.stifftrig(4), np.tile([0.0, 1.0], (4, 1)).astype(np.float64), 0.0, 0.5,
                    1e-6, 1e-6, 1, 1)
     out.append(("stifftrig_sie", "sie", t))

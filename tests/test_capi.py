@@ -66,6 +66,13 @@ def test_global_entry_argument_errors():
     assert w.wind_integrate_global(C.byref(o), C.byref(ks), 0.0, 1.0, 0, yk.ctypes.data, 2, 1e-8,
                                    1e-6, C.byref(tot), C.byref(t), _capi.MEM_HOST,
                                    None) == _capi.WIND_ERR_ARGUMENT
+    # tiled networks are integrated by wind_integrate, not by the shared-step variant
+    kt = W.tile_workload(k, 3)
+    ts = _capi.network_struct(kt.net)
+    yt = kt.y0.copy()
+    assert w.wind_integrate_global(C.byref(o), C.byref(ts), 0.0, 1.0, 1, yt.ctypes.data, 2, 1e-8,
+                                   1e-6, C.byref(tot), C.byref(t), _capi.MEM_HOST,
+                                   None) == _capi.WIND_ERR_UNSUPPORTED
 
 
 def test_defaults_and_strings():
@@ -94,9 +101,15 @@ def test_argument_errors_are_returned():
     ns = _capi.network_struct(net)
     assert w.wind_integrate(C.byref(o), C.byref(ns), 0.0, 1.0, 1, y.ctypes.data, 4, 1e-6, 1e-6,
                             None, None, None, 0, None) == _capi.WIND_ERR_ARGUMENT
-    # wrong equation count for the builtin network
+    # wrong equation count for the builtin network (not a whole number of tiles)
     bad = W.Network(W.NET_NR_TEST, 3, 4, constants=net.constants)
     assert _call(bad, y) == _capi.WIND_ERR_ARGUMENT
+    kc = W.workload_katz96(4).net.constants
+    assert _call(W.Network(W.NET_KATZ96, 12, 4, constants=kc), np.ones((4, 12))) == \
+        _capi.WIND_ERR_ARGUMENT
+    # more tiles than the tiled kernel holds
+    assert _call(W.Network(W.NET_KATZ96, 5 * 65, 4, constants=kc), np.ones((4, 325))) == \
+        _capi.WIND_ERR_UNSUPPORTED
     # missing constants
     bad = W.Network(W.NET_KATZ96, 5, 4)
     assert _call(bad, np.ones((4, 5))) == _capi.WIND_ERR_ARGUMENT

@@ -54,6 +54,33 @@ def test_config3_dense32_full_interval(cuda_device, dense32, solver):
     assert (st & ~8).max() == 0
 
 
+@pytest.mark.parametrize("solver", ["gje_f64", "lu_f64", "mixed"])
+def test_config3_divergent_system_flagged(cuda_device, solver):
+    """System 42 of the dense batch blows up in finite time under the
+    reference algorithm (the oracle ends non-finite); every solver flags it
+    NONFINITE, and the finite system integrated in the same launch keeps the
+    oracle's result."""
+    wl = W.workload_dense(1, first=42)
+    y_o = wl.y0.copy()
+    _, st_o, _ = O.restated(wl.net, y_o, wl.tnow, wl.tend, wl.atol, wl.rtol, "sie", "gold")
+    assert not np.isfinite(y_o).all() and st_o[0] & SYS_NONFINITE
+    w0 = W.workload_dense(1, first=0)
+    y0_o = w0.y0.copy()
+    O.restated(w0.net, y0_o, w0.tnow, w0.tend, w0.atol, w0.rtol, "sie", "gold")
+    both = W.Workload(W._cat_networks([w0.net, wl.net], slice(0, 2)),
+                      np.concatenate([w0.y0, wl.y0]), wl.tnow, wl.tend, wl.atol, wl.rtol, 1, 1,
+                      "dense32")
+    y = both.y0.copy()
+    _, st, _ = lib.integrate(both.net, y, both.tnow, both.tend, both.atol, both.rtol, "sie",
+                             solver, "gold")
+    assert st[1] & SYS_NONFINITE and not np.isfinite(y[1]).all()
+    assert (st[0] & ~8) == 0
+    if solver == "gje_f64":
+        assert np.array_equal(y[0], y0_o[0])
+    else:
+        assert mixed_err(y[:1], y0_o, wl.atol) <= 1e-5
+
+
 # ---- config 4 --------------------------------------------------------------
 @pytest.fixture(scope="module")
 def config4():

@@ -69,3 +69,31 @@ def test_bench_workloads_have_the_named_shapes():
     assert wl.net.n_eq == 64 and wl.net.n_react == 640 and wl.net.nsys == 16
     s = wl.net.species
     assert s.dtype == np.uint16 and int(s.max()) < 64
+
+
+def test_bench_shards_cover_the_dense_job_once():
+    # strong scaling: two ranks' shards are the two halves of the same job
+    full, _ = bench.make_workload("dense", 64, 0.0)
+    parts = [bench.make_workload("dense", 64, 0.0, r, 2)[0] for r in range(2)]
+    assert [p.net.nsys for p in parts] == [32, 32]
+    assert np.array_equal(np.concatenate([p.y0 for p in parts]), full.y0)
+    assert np.array_equal(np.concatenate([p.net.rates for p in parts]), full.net.rates)
+    assert np.array_equal(np.concatenate([p.net.linear for p in parts]), full.net.linear)
+    k = [bench.make_workload("katz96", 10, 0.0, r, 3)[0].net.nsys for r in range(3)]
+    assert k == [4, 3, 3]
+
+
+def test_bench_error_stats_count_divergent_systems():
+    ref = np.array([[1.0, 2.0], [np.nan, 1.0], [1.0, 1.0], [3.0, np.inf]])
+    y = np.array([[1.0, 2.0 + 2e-6], [np.nan, np.nan], [np.nan, 1.0], [3.0, 1.0]])
+    e = bench.error_stats(y, ref, 1e-8)
+    assert abs(e["max_rel_err"] - 1e-6) < 1e-12
+    assert e["finite_systems"] == 1 and e["nonfinite_both"] == 1 and e["finiteness_differs"] == 2
+    assert bench.error_stats(y[1:2], ref[1:2], 1e-8)["max_rel_err"] is None
+
+
+def test_bench_json_is_strict():
+    import json
+    line = bench.finite_json({"a": float("nan"), "b": [1.0, float("inf")], "c": {"d": 2}})
+    assert line == {"a": None, "b": [1.0, None], "c": {"d": 2}}
+    json.dumps(line, allow_nan=False)

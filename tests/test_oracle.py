@@ -144,3 +144,51 @@ def test_global_controller_gives_up_after_nine_refinements():
     assert t_reached == 0.0
     assert np.array_equal(y, wl.y0)
     assert tot == 9 * 3 * 4
+
+
+def test_dense_workload_diverges_under_the_reference_algorithm():
+    """System 42 of the seed-2 dense N=32 workload blows up in finite time at
+    dt = 1 (its random two-body reactions dominate the linear decay): the
+    restated reference algorithm ends non-finite and flags it, as does the
+    reference's own c_baseline build; system 0 stays finite."""
+    for s, finite in ((0, True), (42, False)):
+        wl = W.workload_dense(1, first=s)
+        y = wl.y0.copy()
+        _, st, ns = O.restated(wl.net, y, 0.0, 1.0, 1e-8, 1e-6, "sie", "gold")
+        assert bool(np.isfinite(y).all()) == finite
+        assert (int(st[0]) & 1) == (0 if finite else 1)
+        if O.reference_available(wl.net):
+            yr = wl.y0.copy()
+            tot = O.reference(wl.net, yr, 0.0, 1.0, 1e-8, 1e-6, "sie")
+            assert bool(np.isfinite(yr).all()) == finite
+            if finite:
+                assert np.array_equal(yr, y) and tot == int(ns[0])
+
+
+def test_tiled_identical_tiles_equal_the_untiled_network():
+    """Ntile identical copies (the reference's tileEquations) integrate as the
+    one untiled system does: the block-diagonal elimination of the full
+    matrix leaves every tile on the untiled trajectory, with the same substep
+    counts."""
+    k = W.workload_katz96(6, seed=104)
+    base = W.Workload(k.net, k.y0, 0.0, 1e12, 1e-8, 1e-6, 1, 1)
+    for method in ("sie", "rk2"):
+        y1 = base.y0.copy()
+        _, _, n1 = O.restated(base.net, y1, 0.0, 1e12 if method == "sie" else 1e6, 1e-8, 1e-6,
+                              method, "gold")
+        t = W.tile_workload(base, 4)
+        yt = t.y0.copy()
+        _, _, nt = O.restated(t.net, yt, 0.0, 1e12 if method == "sie" else 1e6, 1e-8, 1e-6,
+                              method, "gold")
+        assert np.array_equal(yt, np.tile(y1, (1, 4)))
+        assert np.array_equal(nt, n1)
+
+
+def test_tiled_network_arguments():
+    k = W.katz96_rates(np.array([1e4]), np.array([1.0]), np.array([1e-13]))
+    bad = W.Network(W.NET_KATZ96, 7, 1, constants=k)  # not a multiple of 5
+    with pytest.raises(ValueError):
+        O.restated(bad, np.zeros((1, 7)), 0.0, 1.0, 1e-8, 1e-6)
+    with pytest.raises(ValueError):
+        W.tile_network(W.tile_network(W.nr_test(1), 2), 2)
+    assert W.tile_network(W.nr_test(3), 5).name == "nr_test_t5"

@@ -65,7 +65,10 @@ wind_status check_network(const wind_network* net, int64_t nsys) {
     }
     const int n = builtin_n(net->kind);
     if (n < 0) return WIND_ERR_ARGUMENT;
-    if (net->n_eq != n) return WIND_ERR_ARGUMENT;
+    // n_eq = Ntile x N: Ntile copies of the network (the Precompiler's
+    // tiling, python/ode_systems/ode_base.py:86-88, 219-281)
+    if (net->n_eq < n || net->n_eq % n != 0) return WIND_ERR_ARGUMENT;
+    if (net->n_eq / n > WIND_MAX_TILES) return WIND_ERR_UNSUPPORTED;
     if (net->n_const < builtin_nc(net->kind)) return WIND_ERR_ARGUMENT;
     if (nsys > 0 && !net->constants) return WIND_ERR_ARGUMENT;
     return WIND_OK;
@@ -78,7 +81,10 @@ wind_status launch_integrate(const wind_options& o_in, const KParams& p, cudaStr
     if (p.nsys == 0) return WIND_OK;
     wind_options o = o_in;
     o.solver = resolve_solver(o.solver, p.kind, p.n_eq);
-    if (p.kind != WIND_NET_MASS_ACTION) return launch_lane(o, p, stream);
+    if (p.kind != WIND_NET_MASS_ACTION) {
+        const int n = builtin_n(p.kind);
+        return p.n_eq == n ? launch_lane(o, p, stream) : launch_tile(o, p, n, stream);
+    }
     if (p.n_eq <= WIND_TEAM_MAX_EQ) return launch_team(o, p, stream);
     // CTA kernels: global scratch for the matrices that do not fit in shared
     // memory, taken from the stream-ordered pool and returned after the launch

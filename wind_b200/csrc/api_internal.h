@@ -36,6 +36,8 @@ wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream
                              bool allow_alloc = true);
 wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream);
 wind_status launch_lane(const wind_options& o, const KParams& p, cudaStream_t stream);
+// Tiled builtin network (n_eq = Ntile x base_n, 1 < Ntile <= WIND_MAX_TILES).
+wind_status launch_tile(const wind_options& o, const KParams& p, int base_n, cudaStream_t stream);
 // A CTA-kernel launch: kernel, shared-memory budget and size, grid, and
 // the per-block global scratch (doubles; 0 = none).
 struct CtaPlan {
@@ -54,6 +56,8 @@ extern std::atomic<int64_t> g_launches;
 // kernels up to 256).
 constexpr int WIND_MAX_EQ = 256;
 constexpr int WIND_TEAM_MAX_EQ = 32;
+// Most copies of a builtin network one tiled system may hold.
+constexpr int WIND_MAX_TILES = 64;
 
 // The name of the last CUDA error this thread mapped to WIND_ERR_CUDA, with
 // the place it was seen (read back through wind_last_error()).

@@ -88,6 +88,10 @@ extern "C" int wind_integrate_global(const wind_options* opt_in, const wind_netw
     wind_status st = check_network(net, nsys);
     if (st != WIND_OK) return st;
     if (net->kind == WIND_NET_MASS_ACTION) return WIND_ERR_UNSUPPORTED;
+    // one thread integrates one whole system here: tiled networks (n_eq =
+    // Ntile x N) go through wind_integrate
+    const int base_n = net->kind == WIND_NET_KATZ96 ? NetKatz96::N : NetNR::N;
+    if (net->n_eq != base_n) return WIND_ERR_UNSUPPORTED;
     if (nsys > 0 && !y) return WIND_ERR_ARGUMENT;
     if (total_nsteps) *total_nsteps = 0;
     if (t_reached) *t_reached = tnow;

@@ -51,16 +51,22 @@ struct NetTrig {
 
 // Katz96 primordial H/He network, cuda/ode_system/ode_gold.c:3-93 and
 // cuda/ode_system/device_dydt.cu:4-114.  J[13] = J[12] is the reference's
-// sign (ode_gold.c:79); it is kept so results match the reference.
+// sign (ode_gold.c:79); it is kept so results match the reference.  The
+// electron density ne is computed once per evaluation (the generated
+// prefix, python/ode_systems/katz96.py:485-500) and passed to the bodies, so
+// a tile of a tiled network can take tile 0's ne with the same arithmetic.
 struct NetKatz96 {
     static constexpr int N = 5;
     static constexpr int NC = 10;
+    template <class Y>
+    __device__ __forceinline__ static xd ne_of(const Y& y) {
+        return y[1] + y[3] + y[4] * 2.0;
+    }
     template <class C, class Y, class F>
-    __device__ __forceinline__ static void rhs(const C& cc, const Y& y, F& f) {
+    __device__ __forceinline__ static void rhs_ne(const C& cc, xd ne, const Y& y, F& f) {
         xd c[10];
 #pragma unroll
         for (int k = 0; k < 10; k++) c[k] = cc[k];
-        xd ne = y[1] + y[3] + y[4] * 2.0;
         f[0] = c[2] * ne * y[1] - (c[0] * ne + c[1]) * y[0];
         f[1] = -c[2] * ne * y[1] + (c[0] * ne + c[1]) * y[0];
         f[2] = (c[7] + c[8]) * ne * y[3] - (c[3] * ne + c[4]) * y[2];
@@ -68,12 +74,11 @@ struct NetKatz96 {
                (c[5] * ne + c[6]) * y[3];
         f[4] = (c[5] * ne + c[6]) * y[3] - c[9] * ne * y[4];
     }
-    template <class C, class Y, class J>
-    __device__ __forceinline__ static void jac(const C& cc, const Y& y, J& M) {
+    template <class C, class J>
+    __device__ __forceinline__ static void jac_ne(const C& cc, xd ne, J& M) {
         xd c[10];
 #pragma unroll
         for (int k = 0; k < 10; k++) c[k] = cc[k];
-        xd ne = y[1] + y[3] + y[4] * 2.0;
         M[0] = -(c[0] * ne + c[1]);
         M[1] = -xd(M[0]);
         M[6] = -c[2] * ne;
@@ -86,6 +91,53 @@ struct NetKatz96 {
         M[24] = -c[9] * ne;
         M[23] = -xd(M[24]);
     }
+    template <class C, class Y, class F>
+    __device__ __forceinline__ static void rhs(const C& cc, const Y& y, F& f) {
+        rhs_ne(cc, ne_of(y), y, f);
+    }
+    template <class C, class Y, class J>
+    __device__ __forceinline__ static void jac(const C& cc, const Y& y, J& M) {
+        jac_ne(cc, ne_of(y), M);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Tiled builtin networks (python/ode_systems/ode_base.py:86-88, 219-281, the
+// Precompiler's Ntile): one system of Ntile x N equations made of Ntile
+// copies of the network, tile t owning equations [tN, tN + N), every tile
+// reading the system's one set of constants; the Jacobian is block diagonal
+// (reindex, ode_base.py:86-88).  Katz96's generated prefix computes ne from
+// equations 1, 3 and 4 -- tile 0 -- and every tile's body uses it
+// (katz96.py:331-448 reindex only the bodies).  TileOf<Net>::Tile is the
+// functor one tile integrates with; for Katz96 it reads ne from constant
+// slot 10, which the kernel fills with tile 0's ne before each evaluation.
+// ---------------------------------------------------------------------------
+struct NetKatz96Tile {
+    static constexpr int N = 5;
+    static constexpr int NC = 11;
+    template <class C, class Y, class F>
+    __device__ __forceinline__ static void rhs(const C& cc, const Y& y, F& f) {
+        NetKatz96::rhs_ne(cc, xd(cc[10]), y, f);
+    }
+    template <class C, class Y, class J>
+    __device__ __forceinline__ static void jac(const C& cc, const Y& y, J& M) {
+        NetKatz96::jac_ne(cc, xd(cc[10]), M);
+    }
+};
+
+template <class Net>
+struct TileOf {
+    using Tile = Net;
+    static constexpr bool coupled = false;
+    template <class Y>
+    __device__ __forceinline__ static double shared(const Y&) { return 0.0; }
+};
+template <>
+struct TileOf<NetKatz96> {
+    using Tile = NetKatz96Tile;
+    static constexpr bool coupled = true;
+    template <class Y>
+    __device__ __forceinline__ static double shared(const Y& y) { return NetKatz96::ne_of(y).v; }
 };
 
 // ---------------------------------------------------------------------------

@@ -231,6 +231,7 @@ __device__ __forceinline__ double warp_lu_solve(const WarpCtx<NMAX, double>& c, 
                                                 double b) {
     const int l = c.l, N = c.N;
     int mystep = (l < N) ? NMAX : -1;
+    double myrcp = 0.0;  // 1 / U_kk of this lane's pivot step
 #pragma unroll
     for (int k = 0; k < NMAX; k++) {
         if (k < N) {
@@ -238,7 +239,10 @@ __device__ __forceinline__ double warp_lu_solve(const WarpCtx<NMAX, double>& c, 
             const int p = 31 - (int)(__reduce_max_sync(c.mask, key) & 31u);
             double* buf = c.pb + (k & 1) * (NMAX + 4);
             if (l == p) {
-                // columns k..NMAX-1 of the pivot row, then its right-hand side
+                // the reciprocal of the pivot (off the other lanes' path),
+                // columns k..NMAX-1 of the pivot row, its right-hand side
+                myrcp = nr_rcp(a[k]);
+                buf[NMAX + 1] = myrcp;
 #pragma unroll
                 for (int t = k & ~1; t < NMAX; t += 2)
                     *reinterpret_cast<double2*>(buf + t) = make_double2(a[t], a[t + 1]);
@@ -248,7 +252,7 @@ __device__ __forceinline__ double warp_lu_solve(const WarpCtx<NMAX, double>& c, 
             }
             __syncwarp(c.mask);
             if (mystep == NMAX) {
-                const double m = a[k] * nr_rcp(buf[k]);
+                const double m = a[k] * buf[NMAX + 1];
 #pragma unroll
                 for (int t = (k + 1) & ~1; t < NMAX; t += 2) {
                     const double2 w = *reinterpret_cast<const double2*>(buf + t);
@@ -266,7 +270,7 @@ __device__ __forceinline__ double warp_lu_solve(const WarpCtx<NMAX, double>& c, 
     for (int i = NMAX - 1; i >= 0; i--) {
         if (i < N) {
             const int p = c.piv[i];
-            double xi = (l == p) ? z * nr_rcp(a[i]) : 0.0;
+            double xi = (l == p) ? z * myrcp : 0.0;
             xi = __shfl_sync(c.mask, xi, c.leader + p);
             if (mystep >= 0 && mystep < i) z = fma(-a[i], xi, z);
             if (l == i) xl = xi;
@@ -291,6 +295,7 @@ __device__ __forceinline__ int warp_gj_invert(const WarpCtx<NMAX, float>& c, flo
             const int p = 31 - (int)(__reduce_max_sync(c.mask, key) & 31u);
             float* buf = c.pb + (k & 1) * (NMAX + 4);
             if (l == p) {
+                buf[NMAX] = nr_rcp(a[k]);  // the pivot's reciprocal, off the others' path
 #pragma unroll
                 for (int t = 0; t < NMAX; t += 4)
                     *reinterpret_cast<float4*>(buf + t) = make_float4(a[t], a[t + 1], a[t + 2], a[t + 3]);
@@ -298,7 +303,7 @@ __device__ __forceinline__ int warp_gj_invert(const WarpCtx<NMAX, float>& c, flo
             }
             __syncwarp(c.mask);
             if (l < N) {
-                const float r = nr_rcp(buf[k]);
+                const float r = buf[NMAX];
                 // pivot row: a <- r a (as (r-1) a + a); others: a <- a - (a_k r) pivot
                 const float alpha = (l == p) ? r - 1.0f : -a[k] * r;
 #pragma unroll

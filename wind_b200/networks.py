@@ -27,6 +27,9 @@ NET_KATZ96 = 2
 NET_STIFFTRIG = 3
 NET_MASS_ACTION = 4
 
+# Equations of one copy of each builtin network.
+BASE_N = {NET_NR_TEST: 2, NET_KATZ96: 5, NET_STIFFTRIG: 2}
+
 NET_NAMES = {NET_NR_TEST: "NR_test", NET_KATZ96: "Katz96",
              NET_STIFFTRIG: "StiffTrig", NET_MASS_ACTION: "MassAction"}
 
@@ -64,8 +67,17 @@ class Network:
         if self.kind == NET_MASS_ACTION:
             lin = "_lin" if self.linear is not None else ""
             return f"ma_n{self.n_eq}_r{self.n_react}{lin}"
-        return {NET_NR_TEST: "nr_test", NET_KATZ96: "katz96",
-                NET_STIFFTRIG: "stifftrig"}[self.kind]
+        base = {NET_NR_TEST: "nr_test", NET_KATZ96: "katz96", NET_STIFFTRIG: "stifftrig"}[self.kind]
+        nt = self.ntile
+        return base if nt == 1 else f"{base}_t{nt}"
+
+    @property
+    def ntile(self) -> int:
+        """Copies of a builtin network in one system (1 for an untiled
+        network and for mass action)."""
+        if self.kind == NET_MASS_ACTION:
+            return 1
+        return self.n_eq // BASE_N[self.kind]
 
     def subset(self, idx) -> "Network":
         """Systems ``idx`` (slice or index array) as a new Network."""
@@ -124,6 +136,26 @@ def stifftrig(nsys: int, freq: float = 6.0) -> Network:
     """StiffTrig with both constants 2*pi*freq (python/ode_systems/stifftrig.py:29-36)."""
     c = np.full((nsys, 2), 2.0 * np.pi * freq)
     return Network(NET_STIFFTRIG, 2, nsys, constants=c)
+
+
+def tile_network(net: Network, ntile: int) -> Network:
+    """The Precompiler's Ntile tiling (python/ode_systems/ode_base.py:86-88,
+    219-281) of a builtin network: each system becomes ntile copies of it
+    (n_eq x ntile equations, block-diagonal Jacobian) sharing the system's
+    constants; Katz96 copies use tile 0's electron density."""
+    if net.kind == NET_MASS_ACTION or net.ntile != 1:
+        raise ValueError("tile an untiled builtin network")
+    if ntile < 1:
+        raise ValueError("ntile >= 1")
+    return Network(net.kind, net.n_eq * ntile, net.nsys, constants=net.constants)
+
+
+def tile_workload(wl: "Workload", ntile: int) -> "Workload":
+    """Tile a builtin workload: the network by tile_network and each system's
+    initial state repeated ntile times (tileEquations, ode_base.py:225-245)."""
+    return dataclasses.replace(wl, net=tile_network(wl.net, ntile),
+                               y0=np.ascontiguousarray(np.tile(wl.y0, (1, ntile))),
+                               label=f"{wl.label}_t{ntile}")
 
 
 def katz96_rates(T: np.ndarray, nH: np.ndarray, uv: np.ndarray) -> np.ndarray:
