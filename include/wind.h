@@ -28,7 +28,19 @@
 #ifndef WIND_H
 #define WIND_H
 
+#ifdef __CUDACC_RTC__
+/* compiled by NVRTC inside a runtime plug-in: no C library headers */
+typedef signed char int8_t;
+typedef short int16_t;
+typedef int int32_t;
+typedef long long int64_t;
+typedef unsigned char uint8_t;
+typedef unsigned short uint16_t;
+typedef unsigned int uint32_t;
+typedef unsigned long long uint64_t;
+#else
 #include <stdint.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -274,6 +286,39 @@ int wind_server_poll(wind_server* srv, int64_t id, double timeout_s, double* y_o
 int wind_server_stats(wind_server* srv, int64_t* out6);
 /* Finishes all submitted work, then frees the server. */
 int wind_server_destroy(wind_server* srv);
+
+/* ---- runtime network plug-ins (NVRTC) ---------------------------------- */
+/* Replaces the reference's build-time Precompiler (python/ode_systems/
+ * ode_base.py:16-123), which splices a network's bodies into the solver
+ * sources and rebuilds lib/sie.so.  `source` is the network as the
+ * reference's host plug-in (cuda/include/ode_gold.h:1-12, the Precompiler's
+ * ode_gold.c output):
+ *     #include "ode_gold.h"
+ *     void calculate_dydt(float tnow, float* equations, float* constants,
+ *                         float* dydt, int Neqn_p_sys);
+ *     void calculate_jacobian(float* equations, float* constants,
+ *                             float* Jacobian);   (transposed, zero-filled)
+ * It is compiled at run time (NVRTC, sm_100a) in FP64 -- `float` is defined
+ * as `double` around it -- with every product rounded before its add, and
+ * linked to the team-per-system Gauss-Jordan integrator.  n_eq <= 64 equations,
+ * n_const constants per system (NUM_CONST in the plug-in); `options` are
+ * extra NVRTC options separated by spaces (e.g. "-DNTILE=4"), or NULL; the
+ * compiler's log is copied into log[log_size] when given.
+ * Returns WIND_ERR_ARGUMENT when the source does not compile and
+ * WIND_ERR_UNSUPPORTED when NVRTC is not available or n_eq > 64. */
+typedef struct wind_plugin wind_plugin;
+int wind_plugin_create(const char* source, int32_t n_eq, int32_t n_const, const char* options,
+                       wind_plugin** out, char* log, int64_t log_size);
+int wind_plugin_destroy(wind_plugin* plugin);
+/* wind_integrate for a plug-in network: constants[nsys*n_const], y[nsys*n_eq];
+ * the solver is the reference's Gauss-Jordan (GJE_F64; AUTO selects it),
+ * either controller, SIE or RK2.  The time passed to calculate_dydt is the
+ * substep's start, as in the reference's c_baseline (sie_gold.c:54-78). */
+int wind_integrate_plugin(const wind_options* opt, wind_plugin* plugin, double tnow, double tend,
+                          int32_t n_integration_steps, const double* constants, double* y,
+                          int64_t nsys, double atol, double rtol, int32_t* sys_status,
+                          int64_t* sys_nsteps, int64_t* total_nsteps, int32_t memory,
+                          void* stream);
 
 /* ---- version / diagnostics -------------------------------------------- */
 const char* wind_version(void);

@@ -138,6 +138,16 @@ def declare_api(lib: C.CDLL) -> C.CDLL:
         C.POINTER(WindOptions), C.POINTER(WindNetwork), C.c_double, C.c_double,
         C.c_int32, P, C.c_int64, C.c_double, C.c_double, P, P, C.c_int32, P]
     lib.wind_integrate_global.restype = C.c_int
+    lib.wind_plugin_create.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_char_p,
+                                       C.POINTER(C.c_void_p), C.c_char_p, C.c_int64]
+    lib.wind_plugin_create.restype = C.c_int
+    lib.wind_plugin_destroy.argtypes = [C.c_void_p]
+    lib.wind_plugin_destroy.restype = C.c_int
+    lib.wind_integrate_plugin.argtypes = [
+        C.POINTER(WindOptions), C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_void_p,
+        C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+        C.c_int32, C.c_void_p]
+    lib.wind_integrate_plugin.restype = C.c_int
     lib.wind_version.restype = C.c_char_p
     lib.wind_status_string.argtypes = [C.c_int]
     lib.wind_status_string.restype = C.c_char_p

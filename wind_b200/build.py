@@ -29,7 +29,12 @@ FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 # translation units of libwind.so
 UNITS = ["api", "batch", "noalloc", "dispatch_lane", "dispatch_team", "dispatch_team8",
          "dispatch_team16", "dispatch_team32", "dispatch_warp", "dispatch_cta", "dispatch_mixed", "server", "global",
-         "dispatch_tile"]
+         "dispatch_tile", "plugin"]
+
+# Kernel sources the runtime plug-ins compile with NVRTC (csrc/plugin.cu),
+# embedded in the library under the names their #include lines use.
+EMBEDDED = [("plugin_kernel.cuh", "csrc/plugin_kernel.cuh"), ("common.cuh", "csrc/common.cuh"),
+            ("../../include/wind.h", "../include/wind.h")]
 
 LEGACY_NETS = {"nr_test": "WIND_NET_NR_TEST", "katz96": "WIND_NET_KATZ96",
                "stifftrig": "WIND_NET_STIFFTRIG"}
@@ -73,18 +78,42 @@ def _run(cmd, log=None):
     return r
 
 
+def _write_embedded():
+    """OBJ/embedded_sources.h: the EMBEDDED files as raw string literals."""
+    out = os.path.join(OBJ, "embedded_sources.h")
+    srcs = [os.path.join(HERE, rel) for _, rel in EMBEDDED]
+    if not _stale(out, srcs + [__file__]):
+        return out, srcs
+    lines = ["// generated by wind_b200/build.py: kernel sources for NVRTC", "#pragma once",
+             "struct EmbeddedSource { const char* name; const char* text; };",
+             "static const EmbeddedSource kEmbedded[] = {"]
+    for (name, _), path in zip(EMBEDDED, srcs):
+        with open(path) as fh:
+            text = fh.read()
+        assert ")WINDSRC\"" not in text
+        lines.append(f'    {{"{name}", R"WINDSRC({text})WINDSRC"}},')
+    lines += ["};", f"static const int kEmbeddedCount = {len(EMBEDDED)};", ""]
+    with open(out, "w") as fh:
+        fh.write("\n".join(lines))
+    return out, srcs
+
+
 def build_native(verbose=False):
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(OBJ, exist_ok=True)
     deps = _deps()
+    emb, emb_srcs = _write_embedded()
     objs, jobs = [], []
     for unit in UNITS:
         obj = os.path.join(OBJ, unit + ".o")
         objs.append(obj)
-        if _stale(obj, sorted(_unit_deps(os.path.join(CSRC, unit + ".cu")))):
+        udeps = sorted(_unit_deps(os.path.join(CSRC, unit + ".cu")))
+        if unit == "plugin":
+            udeps += [emb] + emb_srcs
+        if _stale(obj, udeps):
             if verbose:
                 print(f"nvcc {unit}.cu", flush=True)
-            jobs.append(([NVCC] + FLAGS + ["-c", os.path.join(CSRC, unit + ".cu"), "-o", obj],
+            jobs.append(([NVCC] + FLAGS + ["-I" + OBJ, "-c", os.path.join(CSRC, unit + ".cu"), "-o", obj],
                          os.path.join(OBJ, unit + ".ptxas.log")))
     if jobs:
         import concurrent.futures as cf
@@ -93,7 +122,7 @@ def build_native(verbose=False):
                 f.result()
     libwind = os.path.join(LIB, "libwind.so")
     if _stale(libwind, objs):
-        _run([NVCC] + ARCH + ["-shared"] + objs + ["-o", libwind, "-lcudart"])
+        _run([NVCC] + ARCH + ["-shared"] + objs + ["-o", libwind, "-lcudart", "-ldl"])
     for net, netdef in LEGACY_NETS.items():
         os.makedirs(os.path.join(LIB, net), exist_ok=True)
         # sie.so / rk2.so export cudaIntegrateSystem; sie_host.so exports

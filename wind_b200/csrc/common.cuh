@@ -7,8 +7,10 @@
 // is what the reference's x86-64 build does.  Division is IEEE-correct in both.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <cstdint>
 #include <cuda_runtime.h>
+#endif
 
 #include "../../include/wind.h"
 

@@ -241,5 +241,54 @@ def legacy(network: str, method: str):
     return fn
 
 
+class Plugin:
+    """A runtime network compiled with NVRTC (wind_plugin_create): ``source``
+    is the network in the reference's host plug-in contract
+    (cuda/include/ode_gold.h:1-12; calculate_dydt / calculate_jacobian over
+    ``float``, run in FP64).  ``log`` holds the compiler's output."""
+
+    def __init__(self, source: str, n_eq: int, n_const: int, options: str = ""):
+        lib = load()
+        h = C.c_void_p()
+        buf = C.create_string_buffer(1 << 16)
+        code = lib.wind_plugin_create(source.encode(), n_eq, n_const, options.encode() or None,
+                                      C.byref(h), buf, len(buf))
+        self.log = buf.value.decode(errors="replace")
+        if code != _capi.WIND_OK:
+            raise WindError(code, "wind_plugin_create: " + self.log[-2000:])
+        self.handle, self.n_eq, self.n_const = h, n_eq, n_const
+
+    def close(self):
+        if self.handle:
+            load().wind_plugin_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def integrate(self, constants: np.ndarray, y: np.ndarray, tnow: float, tend: float,
+                  atol: float, rtol: float, method: str = "sie", controller: str = "device",
+                  n_integration_steps: int = 1, max_attempts: int = 0, timeout_s: float = 0.0):
+        """Host arrays: ``constants`` float64 [S, n_const], ``y`` float64 [S, N]
+        updated in place.  Returns (total_substeps, status, nsteps)."""
+        lib = load()
+        nsys = y.shape[0]
+        assert y.dtype == np.float64 and y.flags["C_CONTIGUOUS"] and y.shape[1] == self.n_eq
+        c = np.ascontiguousarray(constants, np.float64)
+        o = options(method, "gje_f64", controller, 0, max_attempts, timeout_s)
+        status = np.zeros(nsys, np.int32)
+        nsteps = np.zeros(nsys, np.int64)
+        total = C.c_int64(0)
+        code = lib.wind_integrate_plugin(C.byref(o), self.handle, tnow, tend, n_integration_steps,
+                                         c.ctypes.data, y.ctypes.data, nsys, atol, rtol,
+                                         status.ctypes.data, nsteps.ctypes.data, C.byref(total),
+                                         _capi.MEM_HOST, None)
+        _check(code, "wind_integrate_plugin")
+        return int(total.value), status, nsteps
+
+
 def launch_count() -> int:
     return int(load().wind_launch_count())
