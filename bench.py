@@ -374,12 +374,20 @@ def run_main(args, wl, desc):
     # ---- MIXED vs LU_F64 on the same first slice under the same device
     # deadline: substeps/s of each at full occupancy (the ratio), and
     # (solver "auto") the headline solver = the faster one
+    # (mass action above 32 species: also MIXED_TC, the same solve with the
+    # inverse's rank updates on the tensor cores -- the A/B of the two)
     results = {}
-    for s in ("mixed", "lu_f64"):
+    compared = ["mixed", "lu_f64"]
+    if net.kind == W.NET_MASS_ACTION and N > 32 and args.method == "sie":
+        compared.append("mixed_tc")
+    for s in compared:
         t, n = timed(s, *b0, timeout_s=args.compare_seconds)
         results[s] = {"substeps_per_s": n / t,
                       "timed": f"slice 0 under a {args.compare_seconds:g} s device deadline"}
     mixed_over_fp64 = results["mixed"]["substeps_per_s"] / results["lu_f64"]["substeps_per_s"]
+    if "mixed_tc" in results:
+        results["mixed_tc"]["over_mixed"] = (results["mixed_tc"]["substeps_per_s"] /
+                                             results["mixed"]["substeps_per_s"])
     main_solver = args.solver if args.solver != "auto" else max(
         cand, key=lambda s: results[s]["substeps_per_s"])
 
@@ -444,7 +452,7 @@ def run_main(args, wl, desc):
                                           "status": status_counts(st_main)}
     outs = {main_solver: y_main}
     per_sys = float(steps_main[b0[0]:b0[1]].mean())
-    for s in ("mixed", "lu_f64"):
+    for s in compared:
         results[s]["systems_per_s"] = results[s]["substeps_per_s"] / per_sys
         results[s]["systems_per_s_definition"] = "substeps/s / mean substeps per system of the main run"
 
@@ -790,7 +798,7 @@ def main():
                     "(profiling runs on a small case; the headline uses the default)")
     ap.add_argument("--dt", type=float, default=0.0, help="interval override (profiling cases)")
     ap.add_argument("--method", default="sie", choices=["sie", "rk2"])
-    ap.add_argument("--solver", default="auto", choices=["auto", "gje_f64", "lu_f64", "mixed"])
+    ap.add_argument("--solver", default="auto", choices=["auto", "gje_f64", "lu_f64", "mixed", "mixed_tc"])
     ap.add_argument("--controller", default="gold", choices=["gold", "device"])
     ap.add_argument("--spec-width", type=int, default=0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)

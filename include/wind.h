@@ -71,8 +71,18 @@ enum {
 
 /* ---- enums --------------------------------------------------------------- */
 /* Integration method: the reference builds one library per method
- * (cuda/Makefile:68-73, -DSIE / -DRK2). */
-enum { WIND_METHOD_SIE = 0, WIND_METHOD_RK2 = 1 };
+ * (cuda/Makefile:68-73, -DSIE / -DRK2).
+ * SIM: the semi-implicit midpoint rule with smoothing step (Bader-Deuflhard,
+ *      Numerical Recipes 16.6) of python/pysolvers/sim.py:36-90 -- FIXED
+ *      steps, no error control: n_integration_steps = m steps of
+ *      h = (tend - tnow)/m, the Jacobian re-evaluated at every step, each
+ *      (I - hJ) solve by the FP64 LU (solver LU_F64 or AUTO; the controller,
+ *      atol, rtol, spec_width and max_attempts are not used).  sys_nsteps
+ *      counts the m + 1 linear solves.  Accepted by wind_integrate for the
+ *      untiled builtin networks and mass-action networks of up to 32
+ *      species; other shapes and the other entry points return
+ *      WIND_ERR_UNSUPPORTED / WIND_ERR_ARGUMENT. */
+enum { WIND_METHOD_SIE = 0, WIND_METHOD_RK2 = 1, WIND_METHOD_SIM = 2 };
 
 /* Step-doubling controller semantics.
  * DEVICE: the reference GPU kernel (cuda/common/kernel.cu:12-39, 191-296):
@@ -103,7 +113,15 @@ enum { WIND_CTRL_DEVICE = 0, WIND_CTRL_GOLD = 1 };
  * AUTO:    per network shape, the faster of the two measured on B200: LU_F64
  *          for the compiled networks and N <= 32, MIXED above 32 species (one
  *          persistent launch still serves a mixed-size batch). */
-enum { WIND_SOLVER_GJE_F64 = 0, WIND_SOLVER_LU_F64 = 1, WIND_SOLVER_MIXED = 2, WIND_SOLVER_AUTO = 3 };
+/* MIXED_TC: MIXED for mass-action networks with 32 < N <= 256 (wind_integrate,
+ *          wind_integrate_output_steps), the blocked inverse's rank-16
+ *          updates on the 5th-generation tensor cores: tcgen05.mma kind::tf32
+ *          with the accumulator in tensor memory, each operand split into
+ *          TF32 high and low parts (hi*hi + hi*lo + lo*hi, FP32-level
+ *          products); rows beyond the first 128 on the CUDA cores.  Other
+ *          shapes and entry points return WIND_ERR_UNSUPPORTED. */
+enum { WIND_SOLVER_GJE_F64 = 0, WIND_SOLVER_LU_F64 = 1, WIND_SOLVER_MIXED = 2, WIND_SOLVER_AUTO = 3,
+       WIND_SOLVER_MIXED_TC = 4 };
 
 /* Network kinds: the ode_system plug-ins (cuda/include/device.h:1-13,
  * cuda/include/ode_gold.h:1-12).

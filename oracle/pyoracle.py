@@ -48,6 +48,10 @@ def _load_oracle():
             C.POINTER(_capi.WindNetwork), C.c_double, C.c_double, C.c_int, P, C.c_int64,
             C.c_double, C.c_double, C.POINTER(C.c_double)]
         lib.wind_oracle_integrate_global.restype = C.c_int64
+        lib.wind_oracle_integrate_sim.argtypes = [
+            C.POINTER(_capi.WindNetwork), C.c_double, C.c_double, C.c_int, P, C.c_int64,
+            C.c_int64, P, P]
+        lib.wind_oracle_integrate_sim.restype = C.c_int64
         lib.wind_oracle_rhs_jac.argtypes = [C.POINTER(_capi.WindNetwork), C.c_int64,
                                             P, P, P]
         lib.wind_oracle_rhs_jac.restype = C.c_int
@@ -107,6 +111,22 @@ def restated_global(net: Network, y: np.ndarray, tnow: float, tend: float, atol:
     if tot < 0:
         raise ValueError("oracle rejected the arguments")
     return int(tot), float(t.value)
+
+
+def restated_sim(net: Network, y: np.ndarray, tnow: float, tend: float, m: int):
+    """The semi-implicit midpoint rule restated (m steps of (tend - tnow)/m
+    and the smoothing step); updates ``y`` in place, returns
+    (total solves, status, nsteps)."""
+    lib = _load_oracle()
+    assert y.dtype == np.float64 and y.flags["C_CONTIGUOUS"]
+    ns = _capi.network_struct(net)
+    status = np.zeros(net.nsys, np.int32)
+    steps = np.zeros(net.nsys, np.int64)
+    tot = lib.wind_oracle_integrate_sim(C.byref(ns), tnow, tend, m, y.ctypes.data, 0, net.nsys,
+                                        status.ctypes.data, steps.ctypes.data)
+    if tot < 0:
+        raise ValueError("oracle rejected the arguments")
+    return int(tot), status, steps
 
 
 def rhs_jac(net: Network, s: int, y: np.ndarray):

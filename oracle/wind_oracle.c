@@ -474,3 +474,89 @@ int64_t wind_oracle_integrate_global(const wind_network* net, double tnow, doubl
     free(y2);
     return nsteps * nsys;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Semi-implicit midpoint rule (Bader-Deuflhard), python/pysolvers/sim.py    */
+/* ------------------------------------------------------------------------ */
+/* Solve (I - h J) x = b in place on b, J in the plug-ins' transposed layout
+ * (Jt[i*N+j] = df_j/dy_i), by an FP64 LU with partial pivoting.  The
+ * reference inverts the matrix with numpy.linalg.inv and multiplies
+ * (sim.py:61-64); both are the same solve up to rounding. */
+static int lu_solve_ih(int n, double h, const double* Jt, double* A, double* b) {
+    for (int r = 0; r < n; r++)
+        for (int c = 0; c < n; c++) A[r * n + c] = (r == c ? 1.0 : 0.0) - h * Jt[c * n + r];
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        double best = fabs(A[k * n + k]);
+        for (int r = k + 1; r < n; r++)
+            if (fabs(A[r * n + k]) > best) { best = fabs(A[r * n + k]); p = r; }
+        if (best == 0.0) return -1;
+        if (p != k) {
+            for (int c = 0; c < n; c++) {
+                double t = A[k * n + c]; A[k * n + c] = A[p * n + c]; A[p * n + c] = t;
+            }
+            double t = b[k]; b[k] = b[p]; b[p] = t;
+        }
+        for (int r = k + 1; r < n; r++) {
+            double m = A[r * n + k] / A[k * n + k];
+            for (int c = k + 1; c < n; c++) A[r * n + c] -= m * A[k * n + c];
+            b[r] -= m * b[k];
+        }
+    }
+    for (int k = n - 1; k >= 0; k--) {
+        double s = b[k];
+        for (int c = k + 1; c < n; c++) s -= A[k * n + c] * b[c];
+        b[k] = s / A[k * n + k];
+    }
+    return 0;
+}
+
+/* m steps of size h = (tend - tnow)/m of the semi-implicit midpoint rule with
+ * the smoothing step (Numerical Recipes 16.6, as sim.py:36-90 implements it,
+ * with the Jacobian re-evaluated at every y_k, sim.py:59):
+ *   D_0 = (I - hJ(y_0))^-1 h f(y_0),                 y_1 = y_0 + D_0
+ *   D_k = D_{k-1} + 2 (I - hJ(y_k))^-1 (h f(y_k) - D_{k-1}),
+ *                                      y_{k+1} = y_k + D_k,  k = 1..m-1
+ *   ybar = y_m + (I - hJ(y_m))^-1 (h f(y_m) - D_{m-1})
+ * ybar is the result at tend.  The reference's integrate_sie(y0, c, dt, tend)
+ * takes M = len(arange(0, tend + dt, dt)) - 1 interior steps after the first
+ * (sim.py:51-80), so its final row equals m = M + 1 steps over (M + 1) dt.
+ * Per system: nsteps = m + 1 linear solves; status NONFINITE when ybar is
+ * not finite.  Returns the solve total of the range, -1 on bad arguments. */
+int64_t wind_oracle_integrate_sim(const wind_network* net, double tnow, double tend, int m,
+                                  double* y, int64_t s_begin, int64_t s_end,
+                                  int32_t* status, int64_t* sys_nsteps) {
+    if (!net_ok(net) || !y || m < 1) return -1;
+    scratch_t* w = (scratch_t*)malloc(sizeof(scratch_t));
+    double* d = (double*)malloc(sizeof(double) * ORACLE_MAXN);
+    if (!w || !d) { free(w); free(d); return -1; }
+    const int n = net->n_eq;
+    const double h = (tend - tnow) / m;
+    int64_t total = 0;
+    for (int64_t s = s_begin; s < s_end; s++) {
+        sysref sr = {net, s};
+        double* ys = y + s * n;
+        int32_t st = 0;
+        for (int k = 0; k <= m; k++) {
+            eval_rhs(&sr, ys, w->f);
+            eval_jac(&sr, ys, w->J);
+            for (int i = 0; i < n; i++) w->out[i] = h * w->f[i] - (k ? d[i] : 0.0);
+            if (lu_solve_ih(n, h, w->J, w->Inv, w->out) != 0) {
+                for (int i = 0; i < n; i++) w->out[i] = NAN;
+            }
+            for (int i = 0; i < n; i++) {
+                if (k == 0 || k == m) d[i] = w->out[i];
+                else d[i] = d[i] + 2.0 * w->out[i];
+                ys[i] = ys[i] + d[i];
+            }
+        }
+        for (int i = 0; i < n; i++)
+            if (!isfinite(ys[i])) st |= WIND_SYS_NONFINITE;
+        if (status) status[s] = st;
+        if (sys_nsteps) sys_nsteps[s] = m + 1;
+        total += m + 1;
+    }
+    free(w);
+    free(d);
+    return total;
+}

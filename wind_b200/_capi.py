@@ -33,19 +33,21 @@ SYS_BAD_INPUT = 32
 
 METHOD_SIE = 0
 METHOD_RK2 = 1
+METHOD_SIM = 2
 CTRL_DEVICE = 0
 CTRL_GOLD = 1
 SOLVER_GJE_F64 = 0
 SOLVER_LU_F64 = 1
 SOLVER_MIXED = 2
+SOLVER_MIXED_TC = 4
 MEM_HOST = 0
 MEM_DEVICE = 1
 
-METHODS = {"sie": METHOD_SIE, "rk2": METHOD_RK2}
+METHODS = {"sie": METHOD_SIE, "rk2": METHOD_RK2, "sim": METHOD_SIM}
 CONTROLLERS = {"device": CTRL_DEVICE, "gold": CTRL_GOLD}
 SOLVER_AUTO = 3
 SOLVERS = {"gje_f64": SOLVER_GJE_F64, "lu_f64": SOLVER_LU_F64, "mixed": SOLVER_MIXED,
-           "auto": SOLVER_AUTO}
+           "auto": SOLVER_AUTO, "mixed_tc": SOLVER_MIXED_TC}
 
 
 class WindNetwork(C.Structure):

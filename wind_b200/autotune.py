@@ -2,7 +2,8 @@
 
 For a workload shape (network kind, N, reactions, dense term, method,
 controller, batch size) it times the candidate configurations -- solver
-(LU_F64 / MIXED, plus the reference GJE_F64 as the accuracy anchor) and,
+(LU_F64 / MIXED / MIXED_TC above 32 species, plus the reference GJE_F64 as
+the accuracy anchor) and,
 for the thread-per-system kernel, the initial lanes per system
 (`spec_width` 1, 2, 4, 8; helpers still join at the tail) -- on the GPU,
 keeps the fastest one whose result stays within `tol` of the FP64
@@ -47,10 +48,16 @@ def _save(db):
 
 
 def tune(wl, method="sie", controller="device", tol=1e-5, sample=0, reps=2, widths=(1, 2, 4, 8),
-         solvers=("lu_f64", "mixed")):
+         solvers=None):
     """Time every candidate on `wl` (or a strided sample of `sample` systems)
-    and return (best, table).  Runs on the current CUDA device."""
+    and return (best, table).  Runs on the current CUDA device.  The default
+    candidates are LU_F64 and MIXED, plus MIXED_TC (the tensor-core rank
+    updates) for SIE on mass-action networks above 32 species."""
     import torch
+    if solvers is None:
+        solvers = ("lu_f64", "mixed")
+        if wl.net.kind == W.NET_MASS_ACTION and wl.net.n_eq > 32 and method == "sie":
+            solvers += ("mixed_tc",)
     dev = torch.device("cuda", torch.cuda.current_device())
     if sample and wl.net.nsys > sample:
         wl = wl.subset(slice(0, wl.net.nsys, max(1, wl.net.nsys // sample)))

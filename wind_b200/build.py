@@ -29,7 +29,7 @@ FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 # translation units of libwind.so
 UNITS = ["api", "batch", "noalloc", "dispatch_lane", "dispatch_team", "dispatch_team8",
          "dispatch_team16", "dispatch_team32", "dispatch_warp", "dispatch_cta", "dispatch_mixed", "server", "global",
-         "dispatch_tile", "plugin"]
+         "dispatch_tile", "plugin", "dispatch_sim"]
 
 # Kernel sources the runtime plug-ins compile with NVRTC (csrc/plugin.cu),
 # embedded in the library under the names their #include lines use.

@@ -79,6 +79,11 @@ wind_status check_network(const wind_network* net, int64_t nsys) {
 wind_status launch_integrate(const wind_options& o_in, const KParams& p, cudaStream_t stream,
                              bool allow_alloc) {
     if (p.nsys == 0) return WIND_OK;
+    if (o_in.method == WIND_METHOD_SIM) return launch_sim(o_in, p, stream);
+    // the tensor-core variant exists for the CTA kernels' MIXED inverse only
+    if (o_in.solver == WIND_SOLVER_MIXED_TC &&
+        (p.kind != WIND_NET_MASS_ACTION || p.n_eq <= WIND_TEAM_MAX_EQ || o_in.method != WIND_METHOD_SIE))
+        return WIND_ERR_UNSUPPORTED;
     wind_options o = o_in;
     o.solver = resolve_solver(o.solver, p.kind, p.n_eq);
     if (p.kind != WIND_NET_MASS_ACTION) {
@@ -142,7 +147,7 @@ int wind_integrate(const wind_options* opt_in, const wind_network* net, double t
     wind_options o;
     if (opt_in) o = *opt_in; else wind_default_options(&o);
     (void)cudaGetLastError();  // an earlier, unrelated error is not this call's
-    if (check_options(o) != WIND_OK) return WIND_ERR_ARGUMENT;
+    if (check_options(o, true) != WIND_OK) return WIND_ERR_ARGUMENT;
     if (nsys < 0 || n_integration_steps < 1) return WIND_ERR_ARGUMENT;
     if (memory != WIND_MEM_HOST && memory != WIND_MEM_DEVICE) return WIND_ERR_ARGUMENT;
     wind_status st = check_network(net, nsys);
@@ -175,7 +180,7 @@ int wind_integrate_output_steps(const wind_options* opt_in, const wind_network* 
     if (opt_in) o = *opt_in; else wind_default_options(&o);
     if (n_output_steps < 1 || n_integration_steps < 1 || nsys < 0) return WIND_ERR_ARGUMENT;
     (void)cudaGetLastError();
-    if (check_options(o) != WIND_OK) return WIND_ERR_ARGUMENT;
+    if (check_options(o, true) != WIND_OK) return WIND_ERR_ARGUMENT;
     if (memory != WIND_MEM_HOST && memory != WIND_MEM_DEVICE) return WIND_ERR_ARGUMENT;
     wind_status st = check_network(net, nsys);
     if (st != WIND_OK) return st;

@@ -15,10 +15,14 @@ wind_status check_network(const wind_network* net, int64_t nsys);
 
 // Range checks of the options every entry point applies: an unknown method,
 // controller or solver is an argument error, never read as a default.
-inline wind_status check_options(const wind_options& o) {
-    if (o.method != WIND_METHOD_SIE && o.method != WIND_METHOD_RK2) return WIND_ERR_ARGUMENT;
+// `sim_ok`: the entry point runs the fixed-step WIND_METHOD_SIM (only
+// wind_integrate and wind_integrate_output_steps do).
+inline wind_status check_options(const wind_options& o, bool sim_ok = false) {
+    if (o.method != WIND_METHOD_SIE && o.method != WIND_METHOD_RK2 &&
+        !(sim_ok && o.method == WIND_METHOD_SIM))
+        return WIND_ERR_ARGUMENT;
     if (o.controller != WIND_CTRL_DEVICE && o.controller != WIND_CTRL_GOLD) return WIND_ERR_ARGUMENT;
-    if (o.solver < WIND_SOLVER_GJE_F64 || o.solver > WIND_SOLVER_AUTO) return WIND_ERR_ARGUMENT;
+    if (o.solver < WIND_SOLVER_GJE_F64 || o.solver > WIND_SOLVER_MIXED_TC) return WIND_ERR_ARGUMENT;
     if (o.spec_width < 0 || o.max_attempts < 0 || !(o.timeout_s >= 0.0)) return WIND_ERR_ARGUMENT;
     return WIND_OK;
 }
@@ -35,6 +39,9 @@ inline int resolve_solver(int solver, int kind, int n_eq) {
 wind_status launch_integrate(const wind_options& o, const KParams& p, cudaStream_t stream,
                              bool allow_alloc = true);
 wind_status launch_team(const wind_options& o, const KParams& p, cudaStream_t stream);
+// The fixed-step semi-implicit midpoint rule (WIND_METHOD_SIM): untiled
+// builtin networks and mass action with N <= 32, FP64 LU solves.
+wind_status launch_sim(const wind_options& o, const KParams& p, cudaStream_t stream);
 wind_status launch_lane(const wind_options& o, const KParams& p, cudaStream_t stream);
 // Tiled builtin network (n_eq = Ntile x base_n, 1 < Ntile <= WIND_MAX_TILES).
 wind_status launch_tile(const wind_options& o, const KParams& p, int base_n, cudaStream_t stream);
@@ -130,6 +137,7 @@ struct IntegrateCall {
         p.tend = tend;
         // cuda/common/harness.cu:80, cuda/c_baseline/sie/sie_gold.c:105
         p.h0 = (tend - tnow) / n_integration_steps;
+        p.n_steps = n_integration_steps;
         p.atol = atol;
         p.rtol = rtol;
         p.nsys = nsys;

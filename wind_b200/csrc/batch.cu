@@ -53,6 +53,7 @@ static wind_status fork_pool(size_t n, ForkPool** out) {
 
 wind_status launch_batch(const wind_options& o, const wind_group* groups, int ngroups,
                          cudaStream_t stream) {
+    if (o.solver == WIND_SOLVER_MIXED_TC) return WIND_ERR_UNSUPPORTED;
     for (int g = 0; g < ngroups; g++) {
         wind_status st = check_network(&groups[g].net, groups[g].nsys);
         if (st != WIND_OK) return st;

@@ -56,6 +56,7 @@ struct KParams {
     unsigned long long* counters;  // [0] work queue, [1] substep total, [2] done
     int64_t max_attempts;
     uint64_t timeout_ns;        // 0 = none
+    int32_t n_steps;            // n_integration_steps (the fixed-step method's m)
 };
 
 // Counter slots in the per-call scratch block.

@@ -45,6 +45,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "tc_sm100.cuh"
 #include "networks.cuh"
 
 namespace wind {
@@ -54,6 +55,7 @@ constexpr int CTA_WARPS = CTA_THREADS / 32;
 constexpr int CTA_MAXN = 256;
 constexpr int CTA_NB = 16;  // LU panel width
 constexpr int CTA_CONV = 14; // misc[] slot: refinement converged (0/1)
+constexpr int CTA_TCPAR = 15; // misc[] slot: phase parity of the tensor-core mbarrier
 
 // A warp's pivot candidate for one panel column: its best row's panel
 // entries and the reciprocal of the entry in the column.
@@ -75,7 +77,7 @@ struct CtaLayout {
     int cols;          // columns that hold data (<= ld, a multiple of 4)
     int esz;           // matrix element size (bytes)
     int nvec;          // FP64 vectors of length N
-    int vec, piv, act, misc, cand, lt, mat, inc_off, inc, rt, spc, bytes;
+    int vec, piv, act, misc, cand, tcs, lt, mat, inc_off, inc, rt, spc, bytes;
     bool mat_in_smem, inc_in_smem, data_in_smem;
     size_t g_mat, g_inc, g_doubles;  // global slot: offsets and size in doubles
     __host__ __device__ static int a16(int x) { return (x + 15) & ~15; }
@@ -90,7 +92,14 @@ struct CtaLayout {
         const int per = 128 / esz, want = 16 / esz;  // elements per bank sweep / per 16 B
         return base + ((want - base % per) + per) % per;
     }
-    __host__ __device__ CtaLayout(int N, int R, bool lin, int solver, int smem_cap) {
+    // Tensor-core staging of the MIXED inverse's rank-16 updates (tc): the
+    // mbarrier and tensor-memory address (64 B), the update's left operand
+    // (128 rows x 16, TF32 high and low parts, 16 KB) and right operand
+    // (columns rounded up to 16 x 16, high and low parts).
+    __host__ __device__ static int tc_stage_bytes(int N) {
+        return 64 + 4 * 4096 + 4 * ((N + 15) & ~15) * 32;
+    }
+    __host__ __device__ CtaLayout(int N, int R, bool lin, int solver, int smem_cap, bool tc = false) {
         esz = (solver == WIND_SOLVER_MIXED) ? 4 : 8;
         ld = row_stride(N, esz);
         cols = data_cols(N);
@@ -101,6 +110,7 @@ struct CtaLayout {
         act = off; off = a16(off + N * 4);
         misc = off; off = a16(off + 2 * CTA_WARPS * 4);
         cand = off; off = a16(off + (solver == WIND_SOLVER_GJE_F64 ? 0 : 2 * CTA_WARPS * (16 + CTA_NB * esz)));
+        tcs = off; off = a16(off + (tc ? tc_stage_bytes(N) : 0));
         lt = off; off = a16(off + (lin ? N * N * 4 : 0));
         const int mbytes = (solver == WIND_SOLVER_GJE_F64) ? 0 : a16(N * ld * esz);
         mat = off;
@@ -144,6 +154,12 @@ struct CtaCtx {
     int* misc;   // warp counts [CTA_WARPS]
     unsigned long long* best;  // pivot vote, three rotating slots
     void* cand;  // CtaCand<T>[2][CTA_WARPS]
+    // tensor-core rank updates (MIXED_TC): accumulator base in tensor
+    // memory, completion mbarrier, operand staging, columns rounded to 16
+    uint32_t tmem;
+    uint64_t* mbar;
+    unsigned char* tcs;
+    int tc_cols16;
 };
 
 // 4 consecutive elements through 16-byte shared/global vectors.
@@ -646,6 +662,153 @@ __device__ __forceinline__ double cta_max_abs(const CtaCtx& c, double v, int& ph
     return (double)__uint_as_float(m);
 }
 
+// A[R][R] -= A[R][P] A[P][R] (P = panel [k0, k0+kb), R the other indices)
+// over 4x4 register tiles of the 4-aligned row and column chunks that miss P,
+// for the row chunks from `rc0` on (0: every row; 32: the rows below the
+// 128 the tensor cores update).
+static __device__ __forceinline__ void cta_rank_update(const CtaCtx& c, float* A, int k0, int kb, int rc0) {
+    const int N = c.N, tid = c.tid, ld = c.ld;
+    const int nch = (N + 3) >> 2;
+    const int pc0 = k0 >> 2, pc1 = (k0 + kb + 3) >> 2;  // chunks touching P
+    const int r_lo = pc0 > rc0 ? pc0 : rc0, r_hi = pc1 > rc0 ? pc1 : rc0;  // P's chunks at or above rc0
+    const int mr = (nch - rc0) - (r_hi - r_lo);  // row chunks to update
+    const int m4 = nch - (pc1 - pc0);            // column chunks outside P
+    for (int t = tid; t < mr * m4; t += CTA_THREADS) {
+        const int ti = t / m4, tj = t - ti * m4;
+        const int ri = rc0 + ti < r_lo ? rc0 + ti : rc0 + ti + (r_hi - r_lo);
+        const int cj = tj < pc0 ? tj : tj + (pc1 - pc0);
+        const int col = 4 * cj;
+        float acc[4][4];
+        int rows[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int i = 4 * ri + r;
+            rows[r] = i < N ? i * ld : -1;
+            if (rows[r] >= 0) ld4(A + rows[r] + col, acc[r]);
+            else acc[r][0] = acc[r][1] = acc[r][2] = acc[r][3] = 0.0f;
+        }
+#pragma unroll 1
+        for (int q0 = 0; q0 < CTA_NB; q0 += 4) {
+            float u[4][4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (q0 + q < kb) ld4(A + (size_t)(k0 + q0 + q) * ld + col, u[q]);
+                else u[q][0] = u[q][1] = u[q][2] = u[q][3] = 0.0f;
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                float l[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                if (rows[r] >= 0) ld4(A + rows[r] + k0 + q0, l);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float lq = (q0 + q < kb) ? l[q] : 0.0f;
+#pragma unroll
+                    for (int cc = 0; cc < 4; cc++) acc[r][cc] = fmaf(-lq, u[q][cc], acc[r][cc]);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            if (rows[r] >= 0) st4(A + rows[r] + col, acc[r]);
+    }
+}
+
+// Step 3 of the blocked inverse on the tensor cores.  The rows [0, M) of
+// A, M = min(N, 128), go into the tensor-memory accumulator (row i = lane i),
+// one kind::tf32 MMA chain adds (-A[R][P]) (A[P][R]) with both operands split
+// into TF32 high and low parts (hi*hi + hi*lo + lo*hi: FP32-level products,
+// the 3xTF32 scheme), and the accumulator is copied back.  Rows of P and
+// columns of P are zero in the operands, so they come back unchanged.  Rows
+// [128, N) are updated on the CUDA cores while the MMAs run.  `par` is the
+// mbarrier's phase parity, flipped once per panel.  A wait that runs out
+// (it never should) leaves those rows un-updated: the inverse is then wrong,
+// the refinement that uses it does not converge, and the substep goes to the
+// pivoted recovery path (flagged WIND_SYS_REFINE_FALLBACK).
+static __device__ __forceinline__ void cta_rank_update_tc(const CtaCtx& c, float* A, int k0, int kb,
+                                                           uint32_t& par) {
+    const int N = c.N, tid = c.tid, ld = c.ld;
+    const int M = N < 128 ? N : 128;
+    const int cols16 = c.tc_cols16;
+    const int w = tid >> 5, lane = tid & 31;
+    const int sub = w & 3, half = w >> 2;          // two warps per lane quarter
+    const int row = sub * 32 + lane;
+    const uint32_t trow = c.tmem + ((uint32_t)(sub * 32) << 16);
+    unsigned char* xs = c.tcs;                     // [hi s0 | hi s1 | lo s0 | lo s1], 4 KB each
+    unsigned char* gs = c.tcs + 4 * 4096;          // same, cols16 * 32 B each
+    const int gsl = cols16 * 32;
+    // (a) rows [0, M) into the accumulator, 16 columns per store
+    for (int c0 = half * 16; c0 < cols16; c0 += 32) {
+        float v[16];
+        const float* src = A + (size_t)(row < M ? row : 0) * ld + c0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            float a4[4];
+            ld4(src + 4 * q, a4);
+#pragma unroll
+            for (int e = 0; e < 4; e++) v[4 * q + e] = row < M ? a4[e] : 0.0f;
+        }
+        tc::tmem_st16(trow + c0, v);
+    }
+    // (b) operands: X = -A[R][P] (rows < M), G = A[P][R] stored by output column
+    for (int t = tid; t < 128 * CTA_NB; t += CTA_THREADS) {
+        const int i = t >> 4, q = t & 15;
+        float x = 0.0f;
+        if (i < M && (i < k0 || i >= k0 + kb) && q < kb) x = -A[(size_t)i * ld + k0 + q];
+        const float hi = tc::to_tf32(x), lo = tc::to_tf32(x - hi);
+        const int off = (q >> 3) * 4096 + tc::slab_off(i, q & 7);
+        *reinterpret_cast<float*>(xs + off) = hi;
+        *reinterpret_cast<float*>(xs + 2 * 4096 + off) = lo;
+    }
+    for (int t = tid; t < cols16 * CTA_NB; t += CTA_THREADS) {
+        const int j = t >> 4, q = t & 15;
+        float g = 0.0f;
+        if (j < N && (j < k0 || j >= k0 + kb) && q < kb) g = A[(size_t)(k0 + q) * ld + j];
+        const float hi = tc::to_tf32(g), lo = tc::to_tf32(g - hi);
+        const int off = (q >> 3) * gsl + tc::slab_off(j, q & 7);
+        *reinterpret_cast<float*>(gs + off) = hi;
+        *reinterpret_cast<float*>(gs + 2 * gsl + off) = lo;
+    }
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+        tc::fence_after_sync();
+        const uint32_t id = tc::idesc_tf32(128, cols16);
+        for (int sl = 0; sl < 2 && 8 * sl < kb; sl++) {
+            const uint64_t xh = tc::smem_desc(tc::smem_u32(xs + sl * 4096));
+            const uint64_t xl = tc::smem_desc(tc::smem_u32(xs + (2 + sl) * 4096));
+            const uint64_t gh = tc::smem_desc(tc::smem_u32(gs + sl * gsl));
+            const uint64_t gl = tc::smem_desc(tc::smem_u32(gs + (2 + sl) * gsl));
+            tc::mma_tf32(c.tmem, xh, gh, id, true);
+            tc::mma_tf32(c.tmem, xh, gl, id, true);
+            tc::mma_tf32(c.tmem, xl, gh, id, true);
+        }
+        tc::mma_commit(c.mbar);
+    }
+    // (c) rows [128, N) on the CUDA cores meanwhile
+    if (N > 128) cta_rank_update(c, A, k0, kb, 32);
+    // (d) the accumulator back into rows [0, M)
+    bool ok = tc::mbar_wait(c.mbar, par, 1u << 24);
+    ok = __all_sync(0xffffffffu, ok);
+    par ^= 1u;
+    tc::fence_after_sync();
+    if (ok) {
+        for (int c0 = half * 16; c0 < cols16; c0 += 32) {
+            float v[16];
+            tc::tmem_ld16(trow + c0, v);
+            if (row < M) {
+                float* dst = A + (size_t)row * ld + c0;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    float a4[4] = {v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]};
+                    st4(dst + 4 * q, a4);
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+}
+
 // Unpivoted blocked Gauss-Jordan inversion of A (N x N, FP32, row stride
 // c.ld, shared memory) in place.  Per panel P = [k0, k0+kb) with the other
 // indices R = [0, N) \ P:
@@ -657,13 +820,17 @@ __device__ __forceinline__ double cta_max_abs(const CtaCtx& c, double v, int& ph
 //  4. A[R][P] <- -A[R][P] D^-1         one thread per row of R.
 // Four CTA barriers per panel.  Without pivoting the diagonal blocks must be
 // invertible; a bad inverse shows up as a refinement that does not converge.
+//
+// TC = true (the MIXED_TC solver) runs step 3 for the first 128 rows on the
+// tensor cores (cta_rank_update_tc) and for the rows below them on the CUDA
+// cores at the same time.
+template <bool TC>
 static __device__ __noinline__ void cta_gj_invert(const CtaCtx& c, float* A) {
     const int N = c.N, tid = c.tid, ld = c.ld;
-    const int nch = (N + 3) >> 2;  // 4-wide chunks holding rows / columns < N
     if (tid < N) c.act[tid] = tid;   // row i expresses unknown i (no pivoting)
+    uint32_t tc_par = TC ? (uint32_t)c.misc[CTA_TCPAR] : 0u;  // mbarrier phase parity
     for (int k0 = 0; k0 < N; k0 += CTA_NB) {
         const int kb = min(CTA_NB, N - k0);
-        const int pc0 = k0 >> 2, pc1 = (k0 + kb + 3) >> 2;  // chunks touching P
         // 1. D^-1 on warp 0
         if (tid < 32) {
             const int lane = tid;
@@ -716,47 +883,12 @@ static __device__ __noinline__ void cta_gj_invert(const CtaCtx& c, float* A) {
             }
         }
         __syncthreads();
-        // 3. rank-kb update of R x R over 4x4 tiles of the chunks missing P
-        {
-            const int m4 = nch - (pc1 - pc0);  // chunks outside P
-            for (int t = tid; t < m4 * m4; t += CTA_THREADS) {
-                const int ti = t / m4, tj = t - ti * m4;
-                const int ri = ti < pc0 ? ti : ti + (pc1 - pc0);
-                const int cj = tj < pc0 ? tj : tj + (pc1 - pc0);
-                const int col = 4 * cj;
-                float acc[4][4];
-                int rows[4];
-#pragma unroll
-                for (int r = 0; r < 4; r++) {
-                    const int i = 4 * ri + r;
-                    rows[r] = i < N ? i * ld : -1;
-                    if (rows[r] >= 0) ld4(A + rows[r] + col, acc[r]);
-                    else acc[r][0] = acc[r][1] = acc[r][2] = acc[r][3] = 0.0f;
-                }
-#pragma unroll 1
-                for (int q0 = 0; q0 < CTA_NB; q0 += 4) {
-                    float u[4][4];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        if (q0 + q < kb) ld4(A + (size_t)(k0 + q0 + q) * ld + col, u[q]);
-                        else u[q][0] = u[q][1] = u[q][2] = u[q][3] = 0.0f;
-                    }
-#pragma unroll
-                    for (int r = 0; r < 4; r++) {
-                        float l[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                        if (rows[r] >= 0) ld4(A + rows[r] + k0 + q0, l);
-#pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            const float lq = (q0 + q < kb) ? l[q] : 0.0f;
-#pragma unroll
-                            for (int cc = 0; cc < 4; cc++) acc[r][cc] = fmaf(-lq, u[q][cc], acc[r][cc]);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-                    if (rows[r] >= 0) st4(A + rows[r] + col, acc[r]);
-            }
+        // 3. rank-kb update of R x R: on the tensor cores for the first 128
+        //    rows (TC), on the CUDA cores for the rest
+        if constexpr (TC) {
+            cta_rank_update_tc(c, A, k0, kb, tc_par);
+        } else {
+            cta_rank_update(c, A, k0, kb, 0);
         }
         __syncthreads();
         // 4. column panel: one thread per row of R
@@ -780,6 +912,7 @@ static __device__ __noinline__ void cta_gj_invert(const CtaCtx& c, float* A) {
         }
         __syncthreads();
     }
+    if (TC && tid == 0) c.misc[CTA_TCPAR] = (int)tc_par;
 }
 
 // Gauss-Jordan inversion of A in place with partial pivoting and no row
@@ -1047,14 +1180,14 @@ __device__ bool cta_substep(const CtaCtx& c, double h, void* mat, double* gM) {
 // The persistent CTA loop over one group's systems (blockDim.x must be
 // CTA_THREADS).  `gscratch` holds one slot of `gstride` >=
 // CtaLayout::g_doubles doubles per block (null when the layout needs none).
-template <int METHOD, int CTRL, int SOLVER>
+template <int METHOD, int CTRL, int SOLVER, bool TC>
 __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_raw, double* gscratch,
                                         size_t gstride, int smem_cap) {
     constexpr int CAP = Cap<METHOD, CTRL>::value;
     const int N = p.n_eq, R = p.n_react, tid = threadIdx.x;
     const bool own = tid < N;
     const bool lin = p.linear != nullptr;
-    const CtaLayout lay(N, R, lin, SOLVER, smem_cap);
+    const CtaLayout lay(N, R, lin, SOLVER, smem_cap, TC);
     CtaCtx c;
     c.N = N;
     c.R = R;
@@ -1091,6 +1224,30 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
     const uint64_t t_start = p.timeout_ns ? global_ns() : 0;
     __shared__ unsigned long long s_ticket;
     __shared__ int s_flag;
+    // MIXED_TC: the accumulator's tensor-memory columns (a power of two
+    // >= 32 covering the columns rounded to 16), held for the whole launch
+    uint32_t tc_ncols = 32;
+    if constexpr (TC) {
+        c.tc_cols16 = (N + 15) & ~15;
+        while ((int)tc_ncols < c.tc_cols16) tc_ncols <<= 1;
+        c.mbar = reinterpret_cast<uint64_t*>(smem_raw + lay.tcs);
+        uint32_t* taddr = reinterpret_cast<uint32_t*>(smem_raw + lay.tcs + 8);
+        c.tcs = smem_raw + lay.tcs + 64;
+        if (tid < 32) tc::tmem_alloc(taddr, tc_ncols);
+        if (tid == 0) {
+            tc::mbar_init(c.mbar, 1);
+            c.misc[CTA_TCPAR] = 0;
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        c.tmem = *taddr;
+    } else {
+        c.tmem = 0;
+        c.mbar = nullptr;
+        c.tcs = nullptr;
+        c.tc_cols16 = 0;
+    }
 
     while (true) {
         if (tid == 0) s_ticket = atomicAdd(&p.counters[CNT_QUEUE], 1ull);
@@ -1200,7 +1357,7 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
                 auto fresh_solve = [&](double hh) {
                     cta_build<float>(c, hh, A);
                     if (hh < h_pivot) {
-                        cta_gj_invert(c, A);
+                        cta_gj_invert<TC>(c, A);
                         if (cta_refine(c, A, hh, 24, 1.0, phase) == CTA_REFINE_OK) return true;
                         h_pivot = hh;
                         cta_build<float>(c, hh, A);
@@ -1278,6 +1435,13 @@ __device__ __forceinline__ void cta_run(const KParams& p, unsigned char* smem_ra
         }
         __syncthreads();
     }
+    if constexpr (TC) {
+        // every MMA was waited for; the columns go back before the CTA exits
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (tid < 32) tc::tmem_dealloc(c.tmem, tc_ncols);
+    }
 }
 
 // Two CTAs per SM for the FP32 factors (the 157-species matrix is ~100 KB).
@@ -1289,11 +1453,13 @@ struct CtaMinBlocks {
     static constexpr int value = SOLVER == WIND_SOLVER_MIXED ? WIND_CTA_MIXED_BLOCKS : 1;
 };
 
-template <int METHOD, int CTRL, int SOLVER>
+// TC = true: MIXED with the inverse's rank updates on the tensor cores
+// (the MIXED_TC solver).
+template <int METHOD, int CTRL, int SOLVER, bool TC = false>
 __global__ void __launch_bounds__(CTA_THREADS, CtaMinBlocks<SOLVER>::value)
     k_cta(const KParams p, double* gscratch, size_t gstride, int smem_cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, gstride, smem_cap);
+    cta_run<METHOD, CTRL, SOLVER, TC>(p, smem_raw, gscratch, gstride, smem_cap);
 }
 
 }  // namespace wind

@@ -17,6 +17,7 @@ static CtaFn cta_by_solver(int solver) {
         switch (solver) {
         case WIND_SOLVER_GJE_F64: return k_cta<METHOD, CTRL, WIND_SOLVER_GJE_F64>;
         case WIND_SOLVER_LU_F64: return k_cta<METHOD, CTRL, WIND_SOLVER_LU_F64>;
+        case WIND_SOLVER_MIXED_TC: return k_cta<METHOD, CTRL, WIND_SOLVER_MIXED, true>;
         default: return k_cta<METHOD, CTRL, WIND_SOLVER_MIXED>;
         }
     }
@@ -61,8 +62,11 @@ static int cta_blocks_per_sm(CtaFn fn, size_t smem) {
     return nb;
 }
 
+// The solver whose layout a launch uses (MIXED_TC is MIXED with the
+// tensor-core staging added).
 static int method_solver(const wind_options& o) {
-    return (o.method == WIND_METHOD_RK2) ? WIND_SOLVER_LU_F64 : o.solver;
+    if (o.method == WIND_METHOD_RK2) return WIND_SOLVER_LU_F64;
+    return o.solver == WIND_SOLVER_MIXED_TC ? WIND_SOLVER_MIXED : o.solver;
 }
 
 // Choose the shared-memory budget (full, or half an SM for the FP32
@@ -71,6 +75,7 @@ static int method_solver(const wind_options& o) {
 wind_status plan_cta(const wind_options& o, const KParams& p, bool allow_global, CtaPlan* out) {
     if (p.n_eq > CTA_MAXN || p.n_react > 65535) return WIND_ERR_UNSUPPORTED;
     const int solver = method_solver(o);
+    const bool tc = o.method == WIND_METHOD_SIE && o.solver == WIND_SOLVER_MIXED_TC;
     CtaFn fn = cta_fn(o.method, o.controller, o.solver);
     int caps[2] = {smem_optin(), 0};
     int ncap = 1;
@@ -82,8 +87,11 @@ wind_status plan_cta(const wind_options& o, const KParams& p, bool allow_global,
     CtaPlan best{};
     int best_score = 0;
     for (int i = 0; i < ncap; i++) {
-        const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, solver, caps[i]);
+        const CtaLayout lay(p.n_eq, p.n_react, p.linear != nullptr, solver, caps[i], tc);
         if (lay.bytes > caps[i]) continue;
+        // the tensor-core staging must sit in shared memory, and the matrix
+        // with it (the MMA operands are built from it every panel)
+        if (tc && !lay.mat_in_smem) continue;
         if (!allow_global && lay.g_doubles > 0) continue;
         const int nb = cta_blocks_per_sm(fn, lay.bytes);
         const int score = nb + (lay.mat_in_smem ? 1000 : 0);

@@ -24,23 +24,41 @@ static WarpFn warp_fn(int ctrl, int solver) {
 
 int warp_nmax(int n) { return n <= 8 ? 8 : (n <= 16 ? 16 : 32); }
 
-size_t warp_smem_bytes(int n, int R, bool lin, int solver) {
+// Shared memory of a block of `threads` threads running teams for N = n.
+size_t warp_smem_bytes(int n, int R, bool lin, int solver, int threads) {
     const int nmax = warp_nmax(n);
-    return (size_t)(WARP_THREADS / nmax) * WarpLayout(nmax, R, lin, solver).bytes;
+    return (size_t)(threads / nmax) * WarpLayout(nmax, R, lin, solver).bytes;
 }
 
-static int warp_blocks_per_sm(WarpFn fn, size_t smem) {
+// Resident blocks per SM of `fn` at `threads` threads and `smem` bytes.
+static int warp_blocks_per_sm(WarpFn fn, int threads, size_t smem) {
     static std::mutex mu;
-    static std::vector<std::pair<std::pair<const void*, size_t>, int>> cache;
+    static std::vector<std::pair<std::pair<const void*, size_t>, std::pair<int, int>>> cache;
     std::lock_guard<std::mutex> g(mu);
     for (auto& e : cache)
-        if (e.first.first == (const void*)fn && e.first.second == smem) return e.second;
+        if (e.first.first == (const void*)fn && e.first.second == smem && e.second.first == threads)
+            return e.second.second;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, WARP_THREADS, smem) != cudaSuccess || nb < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess || nb < 1) {
+        (void)cudaGetLastError();
         nb = 0;
-    cache.push_back({{(const void*)fn, smem}, nb});
+    }
+    cache.push_back({{(const void*)fn, smem}, {threads, nb}});
     return nb;
+}
+
+// Threads per block for 32-lane teams: the teams per block (1..8) that keep
+// the most teams resident per SM, the larger block on a tie.
+static int warp32_threads(WarpFn fn, size_t team_bytes) {
+    int best_t = 4, best_res = -1;
+    for (int t = 8; t >= 1; t--) {
+        const size_t smem = (size_t)t * team_bytes;
+        if (smem > 227 * 1024) continue;
+        const int res = warp_blocks_per_sm(fn, 32 * t, smem) * t;
+        if (res > best_res) { best_res = res; best_t = t; }
+    }
+    return 32 * best_t;
 }
 
 wind_status launch_warp(const wind_options& o, const KParams& p, cudaStream_t stream) {
@@ -48,17 +66,21 @@ wind_status launch_warp(const wind_options& o, const KParams& p, cudaStream_t st
     WarpFn fn = nmax == 8 ? warp_fn<8>(o.controller, o.solver)
               : nmax == 16 ? warp_fn<16>(o.controller, o.solver)
                            : warp_fn<32>(o.controller, o.solver);
-    const size_t smem = warp_smem_bytes(p.n_eq, p.n_react, p.linear != nullptr, o.solver);
+    const int threads = nmax == 32 ? warp32_threads(fn, warp_smem_bytes(p.n_eq, p.n_react,
+                                                                        p.linear != nullptr,
+                                                                        o.solver, 32))
+                                   : WARP_THREADS;
+    const size_t smem = warp_smem_bytes(p.n_eq, p.n_react, p.linear != nullptr, o.solver, threads);
     if (smem > 227 * 1024) return WIND_ERR_UNSUPPORTED;
-    const int nb = warp_blocks_per_sm(fn, smem);
+    const int nb = warp_blocks_per_sm(fn, threads, smem);
     if (nb < 1) return WIND_ERR_UNSUPPORTED;
-    const int teams = WARP_THREADS / nmax;
+    const int teams = threads / nmax;
     const int64_t need = (p.nsys + teams - 1) / teams;
     const int64_t cap = (int64_t)nb * device_sm_count();
     const int grid = (int)(need < cap ? need : cap);
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return launch_status("k_warp shared-memory attribute");
-    fn<<<grid, WARP_THREADS, smem, stream>>>(p);
+    fn<<<grid, threads, smem, stream>>>(p);
     g_launches++;
     return launch_status("k_warp launch");
 }

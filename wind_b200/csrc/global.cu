@@ -83,6 +83,7 @@ extern "C" int wind_integrate_global(const wind_options* opt_in, const wind_netw
     if (opt_in) o = *opt_in; else wind_default_options(&o);
     (void)cudaGetLastError();
     if (check_options(o) != WIND_OK || o.method != WIND_METHOD_SIE) return WIND_ERR_ARGUMENT;
+    if (o.solver == WIND_SOLVER_MIXED_TC) return WIND_ERR_UNSUPPORTED;
     if (nsys < 0 || n_integration_steps < 1) return WIND_ERR_ARGUMENT;
     if (memory != WIND_MEM_HOST && memory != WIND_MEM_DEVICE) return WIND_ERR_ARGUMENT;
     wind_status st = check_network(net, nsys);

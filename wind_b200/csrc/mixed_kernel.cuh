@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(MIXED_THREADS, SOLVER == WIND_SOLVER_GJE_F64 ?
         const KParams p = groups[order[gi]];
         if (p.nsys > 0) {
             constexpr bool REG = METHOD == WIND_METHOD_SIE && SMALL != WIND_SOLVER_GJE_F64;
-            if (p.n_eq > 32) cta_run<METHOD, CTRL, SOLVER>(p, smem_raw, gscratch, gstride, smem_cap);
+            if (p.n_eq > 32) cta_run<METHOD, CTRL, SOLVER, false>(p, smem_raw, gscratch, gstride, smem_cap);
             else if constexpr (REG) {
                 if (p.n_eq > 16) warp_run<32, CTRL, SMALL>(p, smem_raw);
                 else if (p.n_eq > 8) warp_run<16, CTRL, SMALL>(p, smem_raw);

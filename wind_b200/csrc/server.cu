@@ -280,6 +280,13 @@ int wind_server_create(const wind_server_config* cfg, wind_server** out) {
     if (cfg) c = *cfg; else wind_server_default_config(&c);
     if (c.max_inflight < 1 || c.max_inflight > 64 || c.hbm_budget_bytes <= 0 || c.max_waiting < 1)
         return WIND_ERR_ARGUMENT;
+    // the batch kernels' method, solver and controller (no fixed-step SIM)
+    wind_options oc;
+    wind_default_options(&oc);
+    oc.method = c.method;
+    oc.solver = c.solver;
+    oc.controller = c.controller;
+    if (check_options(oc) != WIND_OK || oc.solver == WIND_SOLVER_MIXED_TC) return WIND_ERR_ARGUMENT;
     if (c.poll_us <= 0) c.poll_us = 200;
     Server* S = new Server();
     S->cfg = c;

@@ -443,6 +443,63 @@ __device__ __noinline__ double warp_fp64_fallback(const WarpCtx<NMAX, float>& cf
 
 // ---------------------------------------------------------------------------
 // The persistent team loop over one group's systems.
+// Stage system s's network in the team's shared-memory slice: rates and
+// species (a species index >= N marks the system BAD_INPUT and is replaced by
+// 0 so every later access stays in bounds), the per-species incidence lists,
+// and the dense term transposed.  Returns true for BAD_INPUT.
+template <int NMAX, typename T>
+__device__ __forceinline__ bool warp_stage_system(const WarpCtx<NMAX, T>& c, const KParams& p,
+                                                  int64_t s, double* rates_s, uint16_t* sp_s,
+                                                  int* inc_off, uint16_t* inc, float* LT) {
+    const int N = c.N, R = c.R, l = c.l;
+    const bool lin = LT != nullptr;
+    // stage the system's network; a species index >= N marks the system
+    // BAD_INPUT and is replaced by 0 so every later access stays in bounds
+    bool bad_idx = false;
+    for (int r = l; r < R; r += NMAX) {
+        rates_s[r] = p.rates[s * R + r];
+        uint2 q = *reinterpret_cast<const uint2*>(p.species + (s * R + r) * 4);
+        const unsigned nn = (unsigned)N;
+        if ((q.x & 0xffffu) >= nn || (q.x >> 16) >= nn || (q.y & 0xffffu) >= nn || (q.y >> 16) >= nn) {
+            bad_idx = true;
+            q = make_uint2(0u, 0u);
+        }
+        *reinterpret_cast<uint2*>(sp_s + 4 * r) = q;
+    }
+    bad_idx = __any_sync(c.mask, bad_idx);
+    __syncwarp(c.mask);
+    // per-species incidence lists (reaction ids ascending)
+    if (l < N) {
+        int cnt = 0;
+        for (int r = 0; r < R; r++) {
+            const uint2 q = *reinterpret_cast<const uint2*>(sp_s + 4 * r);
+            cnt += ((q.x & 0xffff) == (unsigned)l) | ((q.x >> 16) == (unsigned)l) |
+                   ((q.y & 0xffff) == (unsigned)l) | ((q.y >> 16) == (unsigned)l);
+        }
+        inc_off[l + 1] = cnt;
+    }
+    __syncwarp(c.mask);
+    if (l == 0) {
+        inc_off[0] = 0;
+        for (int j = 0; j < N; j++) inc_off[j + 1] += inc_off[j];
+    }
+    __syncwarp(c.mask);
+    if (l < N) {
+        int o = inc_off[l];
+        for (int r = 0; r < R; r++) {
+            const uint2 q = *reinterpret_cast<const uint2*>(sp_s + 4 * r);
+            if ((q.x & 0xffff) == (unsigned)l || (q.x >> 16) == (unsigned)l ||
+                (q.y & 0xffff) == (unsigned)l || (q.y >> 16) == (unsigned)l)
+                inc[o++] = (uint16_t)r;
+        }
+    }
+    if (lin && l < N) {
+        const float* Lg = p.linear + s * (int64_t)N * N;
+        for (int k = 0; k < N; k++) LT[k * NMAX + l] = Lg[l * N + k];
+    }
+    return bad_idx;
+}
+
 template <int NMAX, int CTRL, int SOLVER>
 __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_raw) {
     using T = typename std::conditional<SOLVER == WIND_SOLVER_MIXED, float, double>::type;
@@ -485,50 +542,7 @@ __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_r
         const int64_t s = (int64_t)ticket;
         if (s >= p.nsys) break;
 
-        // stage the system's network; a species index >= N marks the system
-        // BAD_INPUT and is replaced by 0 so every later access stays in bounds
-        bool bad_idx = false;
-        for (int r = l; r < R; r += NMAX) {
-            rates_s[r] = p.rates[s * R + r];
-            uint2 q = *reinterpret_cast<const uint2*>(p.species + (s * R + r) * 4);
-            const unsigned nn = (unsigned)N;
-            if ((q.x & 0xffffu) >= nn || (q.x >> 16) >= nn || (q.y & 0xffffu) >= nn || (q.y >> 16) >= nn) {
-                bad_idx = true;
-                q = make_uint2(0u, 0u);
-            }
-            *reinterpret_cast<uint2*>(sp_s + 4 * r) = q;
-        }
-        bad_idx = __any_sync(c.mask, bad_idx);
-        __syncwarp(c.mask);
-        // per-species incidence lists (reaction ids ascending)
-        if (l < N) {
-            int cnt = 0;
-            for (int r = 0; r < R; r++) {
-                const uint2 q = *reinterpret_cast<const uint2*>(sp_s + 4 * r);
-                cnt += ((q.x & 0xffff) == (unsigned)l) | ((q.x >> 16) == (unsigned)l) |
-                       ((q.y & 0xffff) == (unsigned)l) | ((q.y >> 16) == (unsigned)l);
-            }
-            inc_off[l + 1] = cnt;
-        }
-        __syncwarp(c.mask);
-        if (l == 0) {
-            inc_off[0] = 0;
-            for (int j = 0; j < N; j++) inc_off[j + 1] += inc_off[j];
-        }
-        __syncwarp(c.mask);
-        if (l < N) {
-            int o = inc_off[l];
-            for (int r = 0; r < R; r++) {
-                const uint2 q = *reinterpret_cast<const uint2*>(sp_s + 4 * r);
-                if ((q.x & 0xffff) == (unsigned)l || (q.x >> 16) == (unsigned)l ||
-                    (q.y & 0xffff) == (unsigned)l || (q.y >> 16) == (unsigned)l)
-                    inc[o++] = (uint16_t)r;
-            }
-        }
-        if (lin && l < N) {
-            const float* Lg = p.linear + s * (int64_t)N * N;
-            for (int k = 0; k < N; k++) LT[k * NMAX + l] = Lg[l * N + k];
-        }
+        const bool bad_idx = warp_stage_system(c, p, s, rates_s, sp_s, inc_off, inc, LT);
         // padding of the permuted right-hand side stays zero
         c.qf[l] = (T)0;
         double y = (l < N) ? p.y[s * N + l] : 0.0;
@@ -672,8 +686,21 @@ __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_r
     }
 }
 
+// Block shape of k_warp.  8- and 16-lane teams run four to a 128-thread
+// block.  A 32-lane team (N = 17..32) holds ~16 KB of shared memory, so the
+// teams per block of a launch (1..8, up to `threads`) are chosen on the host
+// for the most resident teams per SM: with four-team blocks a 16 KB team
+// stops at 12 per SM, with seven-team blocks at 14 (each block also costs
+// the 1 KB the runtime reserves).  Both shapes keep the 128-register cap.
+template <int NMAX>
+struct WarpBlock {
+    static constexpr int threads = NMAX == 32 ? 256 : WARP_THREADS;
+    static constexpr int min_blocks = 65536 / 128 / threads;
+};
+
 template <int NMAX, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(WARP_THREADS, 4) k_warp(const KParams p) {
+__global__ void __launch_bounds__(WarpBlock<NMAX>::threads, WarpBlock<NMAX>::min_blocks)
+    k_warp(const KParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     warp_run<NMAX, CTRL, SOLVER>(p, smem_raw);
 }
