@@ -113,13 +113,17 @@ enum { WIND_CTRL_DEVICE = 0, WIND_CTRL_GOLD = 1 };
  * AUTO:    per network shape, the faster of the two measured on B200: LU_F64
  *          for the compiled networks and N <= 32, MIXED above 32 species (one
  *          persistent launch still serves a mixed-size batch). */
-/* MIXED_TC: MIXED for mass-action networks with 32 < N <= 256 (wind_integrate,
+/* MIXED_TC: MIXED for mass-action networks with 32 < N (wind_integrate,
  *          wind_integrate_output_steps), the blocked inverse's rank-16
  *          updates on the 5th-generation tensor cores: tcgen05.mma kind::tf32
  *          with the accumulator in tensor memory, each operand split into
  *          TF32 high and low parts (hi*hi + hi*lo + lo*hi, FP32-level
- *          products); rows beyond the first 128 on the CUDA cores.  Other
- *          shapes and entry points return WIND_ERR_UNSUPPORTED. */
+ *          products); rows beyond the first 128 on the CUDA cores.  The FP32
+ *          matrix and the operand staging must fit in one CTA's shared
+ *          memory together (N up to ~190).  Other shapes and entry points
+ *          return WIND_ERR_UNSUPPORTED.  Measured slower than MIXED on B200
+ *          (the operand staging and the halved CTAs per SM cost more than
+ *          the update it moves off the CUDA cores); AUTO never picks it. */
 enum { WIND_SOLVER_GJE_F64 = 0, WIND_SOLVER_LU_F64 = 1, WIND_SOLVER_MIXED = 2, WIND_SOLVER_AUTO = 3,
        WIND_SOLVER_MIXED_TC = 4 };
 

@@ -31,10 +31,11 @@ def test_mixed_tc_config4_classes_vs_oracle(cuda_device, n):
     assert (st & ~_capi.SYS_REFINE_FALLBACK).max() == 0
 
 
-@pytest.mark.parametrize("n", [40, 100, 130, 200])
+@pytest.mark.parametrize("n", [40, 100, 130, 176])
 def test_mixed_tc_edge_sizes_vs_lu_f64(cuda_device, n):
     """Sizes that are not multiples of 16 (a partial last panel), above 128
-    (rows split between tensor and CUDA cores) and near the 256 limit,
+    (rows split between tensor and CUDA cores) and near the largest size
+    whose matrix and operand staging fit in shared memory together,
     against the plain FP64 path on the same systems (the FP64 LU is checked
     against the oracle by the configuration tests)."""
     wl = W.workload_mixed_class(n, 64, seed=41, dt=1e-4, atol=1e-8, rtol=1e-6)
@@ -59,6 +60,12 @@ def test_mixed_tc_matches_simt_mixed_closely(cuda_device):
 
 
 def test_mixed_tc_unsupported_elsewhere(cuda_device):
+    # above ~190 species the FP32 matrix and the operand staging no longer
+    # fit in one CTA's shared memory together
+    huge = W.workload_mixed_class(220, 2, seed=45)
+    with pytest.raises(lib.WindError) as e:
+        lib.integrate(huge.net, huge.y0.copy(), 0.0, 1e-6, 1e-8, 1e-6, "sie", "mixed_tc", "gold")
+    assert e.value.code == _capi.WIND_ERR_UNSUPPORTED
     small = W.workload_mixed_class(16, 4, seed=43)
     with pytest.raises(lib.WindError) as e:
         lib.integrate(small.net, small.y0.copy(), 0.0, 1e-3, 1e-8, 1e-6, "sie", "mixed_tc", "gold")

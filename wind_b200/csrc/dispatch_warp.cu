@@ -48,28 +48,12 @@ static int warp_blocks_per_sm(WarpFn fn, int threads, size_t smem) {
     return nb;
 }
 
-// Threads per block for 32-lane teams: the teams per block (1..8) that keep
-// the most teams resident per SM, the larger block on a tie.
-static int warp32_threads(WarpFn fn, size_t team_bytes) {
-    int best_t = 4, best_res = -1;
-    for (int t = 8; t >= 1; t--) {
-        const size_t smem = (size_t)t * team_bytes;
-        if (smem > 227 * 1024) continue;
-        const int res = warp_blocks_per_sm(fn, 32 * t, smem) * t;
-        if (res > best_res) { best_res = res; best_t = t; }
-    }
-    return 32 * best_t;
-}
-
 wind_status launch_warp(const wind_options& o, const KParams& p, cudaStream_t stream) {
     const int nmax = warp_nmax(p.n_eq);
     WarpFn fn = nmax == 8 ? warp_fn<8>(o.controller, o.solver)
               : nmax == 16 ? warp_fn<16>(o.controller, o.solver)
                            : warp_fn<32>(o.controller, o.solver);
-    const int threads = nmax == 32 ? warp32_threads(fn, warp_smem_bytes(p.n_eq, p.n_react,
-                                                                        p.linear != nullptr,
-                                                                        o.solver, 32))
-                                   : WARP_THREADS;
+    const int threads = WARP_THREADS;
     const size_t smem = warp_smem_bytes(p.n_eq, p.n_react, p.linear != nullptr, o.solver, threads);
     if (smem > 227 * 1024) return WIND_ERR_UNSUPPORTED;
     const int nb = warp_blocks_per_sm(fn, threads, smem);

@@ -686,21 +686,8 @@ __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_r
     }
 }
 
-// Block shape of k_warp.  8- and 16-lane teams run four to a 128-thread
-// block.  A 32-lane team (N = 17..32) holds ~16 KB of shared memory, so the
-// teams per block of a launch (1..8, up to `threads`) are chosen on the host
-// for the most resident teams per SM: with four-team blocks a 16 KB team
-// stops at 12 per SM, with seven-team blocks at 14 (each block also costs
-// the 1 KB the runtime reserves).  Both shapes keep the 128-register cap.
-template <int NMAX>
-struct WarpBlock {
-    static constexpr int threads = NMAX == 32 ? 256 : WARP_THREADS;
-    static constexpr int min_blocks = 65536 / 128 / threads;
-};
-
 template <int NMAX, int CTRL, int SOLVER>
-__global__ void __launch_bounds__(WarpBlock<NMAX>::threads, WarpBlock<NMAX>::min_blocks)
-    k_warp(const KParams p) {
+__global__ void __launch_bounds__(WARP_THREADS, 4) k_warp(const KParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     warp_run<NMAX, CTRL, SOLVER>(p, smem_raw);
 }
