@@ -364,12 +364,15 @@ def run_main(args, wl, desc):
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) * 1e-3, n
 
-    # ---- warm-up (untimed): W launches of each fast solver on a few systems
+    # ---- warm-up (untimed): W launches of each fast solver on a few systems,
+    # each cut by a 0.25 s device deadline (module load, occupancy and
+    # allocator caches; a few slow systems would otherwise hold a warm-up
+    # launch for tens of seconds)
     b0 = bounds[0]
     cand = ["mixed", "lu_f64"] if args.solver == "auto" else [args.solver]
     for s in cand:
         for i in range(args.warmup):
-            timed(s, b0[0], min(b0[1], b0[0] + 1024))
+            timed(s, b0[0], min(b0[1], b0[0] + 1024), timeout_s=0.25)
 
     # ---- MIXED vs LU_F64 on the same first slice under the same device
     # deadline: substeps/s of each at full occupancy (the ratio), and
@@ -642,6 +645,33 @@ def katz96_extra(args, torch, dev, lib, _capi, C):
             if i:
                 ts.append(e0.elapsed_time(e1) * 1e-3)
         out[solver] = {"systems_per_s": net.nsys / statistics.median(ts), "substeps": int(tot.value)}
+    # the reference caller's own path: the mangled cudaIntegrateSystem of
+    # lib/katz96/sie.so on pageable float32 NumPy arrays (python/wind_harness.py:32-40,
+    # python/ode_systems/ode_base.py:441-469), wall clock around the call
+    try:
+        fn = lib.legacy("katz96", "sie")
+        c32 = np.ascontiguousarray(net.constants, dtype=np.float32)
+        drop = {}
+        for solver in ("gje_f64", "lu_f64"):
+            os.environ["WIND_LEGACY_SOLVER"] = solver
+            ts = []
+            for i in range(3):
+                y32 = np.ascontiguousarray(wl.y0, dtype=np.float32)
+                t0 = time.perf_counter()
+                n = fn(0.0, 1e13, 1, c32.ctypes.data, y32.ctypes.data, net.nsys, 5, 1e-8, 1e-6)
+                if i:
+                    ts.append(time.perf_counter() - t0)
+                if n < 0:
+                    raise RuntimeError(f"cudaIntegrateSystem returned {n}")
+            drop[solver] = {"systems_per_s": net.nsys / statistics.median(ts)}
+        os.environ.pop("WIND_LEGACY_SOLVER", None)
+        drop["call"] = ("_Z19cudaIntegrateSystemffiPfS_iiff from lib/katz96/sie.so, pageable "
+                        "float32 host arrays, wall clock per call (host conversions, copies and "
+                        "the integration)")
+        out["e2e_dropin"] = drop
+    except Exception as exc:  # the headline line must still print
+        os.environ.pop("WIND_LEGACY_SOLVER", None)
+        out["e2e_dropin"] = {"error": str(exc)}
     out["workload"] = "Katz96 5-species, 65,536 cells (seed 1), dt=1e13 s, atol=1e-8 rtol=1e-6"
     return out
 
@@ -803,7 +833,7 @@ def main():
     ap.add_argument("--spec-width", type=int, default=0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--gje-seconds", type=float, default=3.0)
-    ap.add_argument("--e2e-systems", type=int, default=65536,
+    ap.add_argument("--e2e-systems", type=int, default=16384,
                     help="systems of the end-to-end (host buffer) measurement")
     ap.add_argument("--e2e-calls", type=int, default=8,
                     help="concurrent wind_integrate calls the end-to-end systems are split into")

@@ -131,3 +131,22 @@ def test_zero_systems_is_a_no_op():
     assert _call(net, np.ones((0, 2))) == _capi.WIND_OK
     w = lib.load()
     assert w.wind_integrate_batch(C.byref(lib.options()), None, 0, None) == _capi.WIND_OK
+
+
+def test_sim_and_tensor_core_options_are_checked_before_any_work():
+    """The fixed-step SIM method is accepted by wind_integrate only, and the
+    tensor-core solver value is in range; both are rejected by the batch and
+    serving entry points before anything is launched."""
+    w = lib.load()
+    o = lib.options("sim", "lu_f64", "gold")
+    assert o.method == _capi.METHOD_SIM
+    # batch entry points reject the method (no groups are read)
+    assert w.wind_integrate_batch(C.byref(o), None, 0, None) == _capi.WIND_ERR_ARGUMENT
+    o = lib.options("sie", "mixed_tc", "gold")
+    assert o.solver == _capi.SOLVER_MIXED_TC
+    o.solver = _capi.SOLVER_MIXED_TC + 1
+    net = W.nr_test(4)
+    ns = _capi.network_struct(net)
+    y = np.ones((4, 2))
+    assert w.wind_integrate(C.byref(o), C.byref(ns), 0.0, 1.0, 1, y.ctypes.data, 4, 1e-6, 1e-6,
+                            None, None, None, 0, None) == _capi.WIND_ERR_ARGUMENT

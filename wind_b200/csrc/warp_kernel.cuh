@@ -279,6 +279,17 @@ __device__ __forceinline__ double warp_lu_solve(const WarpCtx<NMAX, double>& c, 
     return xl;
 }
 
+// I - hJ from the scatter rows, solved by the FP64 LU, as one out-of-line
+// body: the three solves of an attempt share its instructions (inlined, each
+// was its own copy of the unrolled elimination, and the kernel stalled on
+// instruction fetch).
+template <int NMAX>
+__device__ __noinline__ double warp_lu_solve_at(const WarpCtx<NMAX, double> c, double h, double b) {
+    double a[NMAX];
+    warp_load_matrix(c, h, a);
+    return warp_lu_solve(c, a, b);
+}
+
 // ---- FP32 Gauss-Jordan inverse --------------------------------------------
 // In-place inversion of A (row l in a[]) with partial pivoting and no row
 // exchanges: after step k the pivot lane's row expresses unknown k.  The
@@ -625,11 +636,9 @@ __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_r
                 x = mixed_fresh(h1, fy, true);
                 vh = y + h1 * x;
             } else {
-                warp_load_matrix(c, hf, a);
-                y1 = y + hf * warp_lu_solve(c, a, fy);
+                y1 = y + hf * warp_lu_solve_at(c, hf, fy);
                 __syncwarp(c.mask);
-                warp_load_matrix(c, h1, a);
-                vh = y + h1 * warp_lu_solve(c, a, fy);
+                vh = y + h1 * warp_lu_solve_at(c, h1, fy);
             }
             // ---- second half step from vh
             __syncwarp(c.mask);
@@ -653,8 +662,7 @@ __device__ __forceinline__ void warp_run(const KParams& p, unsigned char* smem_r
                 warp_jma_row(c);
                 jy_ok = false;
                 __syncwarp(c.mask);
-                warp_load_matrix(c, h2, a);
-                y2 = vh + h2 * warp_lu_solve(c, a, f2);
+                y2 = vh + h2 * warp_lu_solve_at(c, h2, f2);
             }
             bool err = false;
             if (l < N) err = elem_error<WIND_METHOD_SIE, CTRL>(xd(y1), xd(y2), p.atol, p.rtol);
