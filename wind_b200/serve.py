@@ -180,4 +180,4 @@ def poisson_load(server: Server, requests, rate_hz: float, seed: int = 4, timeou
     return {"requests": len(requests), "rate_hz": rate_hz, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
             "p99_ms": 1e3 * float(np.percentile(lat, 99)), "mean_ms": 1e3 * float(lat.mean()),
             "systems_per_s": cells / wall, "wall_s": wall, "cells": int(cells),
-            "failed": int(sum(int(r.status.max() != 0) for r in results))}, results
+            "flagged": int(sum(int(r.status.max() != 0) for r in results))}, results
