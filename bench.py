@@ -467,17 +467,19 @@ def run_main(args, wl, desc):
                                                    "substeps per system of the main run")}
     mixed_over_gje = results["mixed"]["substeps_per_s"] / results["gje_f64"]["substeps_per_s"]
 
-    # ---- e2e through the C ABI with pinned host buffers: the first
-    # --e2e-systems systems as --e2e-calls concurrent wind_integrate calls
-    # (host memory mode: each uploads its inputs, integrates and downloads
-    # its state on its own stream, from its own host thread -- ctypes
-    # releases the GIL), so one call's slowest systems overlap the others'
-    # work as in the resident run.  Device time: an event before every
-    # call's upload to an event after every call's download.
-    e2e_lo, e2e_hi = 0, min(S, args.e2e_systems)
+    # ---- e2e through the C ABI with pinned host buffers: by default the
+    # whole job again, as K concurrent wind_integrate calls over the same
+    # slices as the resident run (host memory mode: each uploads its inputs,
+    # integrates and downloads its state on its own stream, from its own
+    # host thread -- ctypes releases the GIL), so one call's slowest systems
+    # overlap the others' work as in the resident run; --e2e-systems /
+    # --e2e-calls select a smaller sample.  Device time: an event before
+    # every call's upload to an event after every call's download.
+    e2e_lo, e2e_hi = 0, min(S, args.e2e_systems) if args.e2e_systems > 0 else S
+    n_calls = args.e2e_calls if args.e2e_calls > 0 else len(bounds)
     e2e_calls = [(int(a0), int(a1)) for a0, a1 in zip(
-        np.linspace(e2e_lo, e2e_hi, args.e2e_calls + 1).round()[:-1],
-        np.linspace(e2e_lo, e2e_hi, args.e2e_calls + 1).round()[1:]) if a1 > a0]
+        np.linspace(e2e_lo, e2e_hi, n_calls + 1).round()[:-1],
+        np.linspace(e2e_lo, e2e_hi, n_calls + 1).round()[1:]) if a1 > a0]
     h_arr = {k: torch.from_numpy(np.ascontiguousarray(getattr(net, k)[e2e_lo:e2e_hi])).pin_memory()
              for k in keys}
     h_y0 = torch.from_numpy(np.ascontiguousarray(wl.y0[e2e_lo:e2e_hi])).pin_memory()
@@ -605,7 +607,9 @@ def run_main(args, wl, desc):
             "mixed_over_gje_f64": mixed_over_gje,
             "max_rel_err_vs_reference": errs or None,
             "e2e": {"value": e2e_job / e2e_tot, "unit": "systems/s",
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "h2d_bytes_per_step": int(h2d / len(e2e_calls)),
+                    "d2h_bytes_per_step": int(d2h / len(e2e_calls)),
+                    "h2d_bytes_total": int(h2d), "d2h_bytes_total": int(d2h),
                     "systems": e2e_sys, "calls": len(e2e_calls),
                     "step": (f"systems 0..{e2e_sys - 1} as {len(e2e_calls)} concurrent "
                              "wind_integrate calls on host buffers, one stream each"),
@@ -833,10 +837,11 @@ def main():
     ap.add_argument("--spec-width", type=int, default=0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--gje-seconds", type=float, default=3.0)
-    ap.add_argument("--e2e-systems", type=int, default=16384,
+    ap.add_argument("--e2e-systems", type=int, default=0,
                     help="systems of the end-to-end (host buffer) measurement")
-    ap.add_argument("--e2e-calls", type=int, default=8,
-                    help="concurrent wind_integrate calls the end-to-end systems are split into")
+    ap.add_argument("--e2e-calls", type=int, default=0,
+                    help="concurrent wind_integrate calls the end-to-end systems are split "
+                         "into (0: one per timed step, as the resident run)")
     ap.add_argument("--compare-seconds", type=float, default=4.0,
                     help="device deadline of the MIXED and LU_F64 rate runs on slice 0")
     ap.add_argument("--traffic-per-system", type=float, default=0.0,

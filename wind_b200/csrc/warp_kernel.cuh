@@ -283,11 +283,28 @@ __device__ __forceinline__ double warp_lu_solve(const WarpCtx<NMAX, double>& c, 
 // body: the three solves of an attempt share its instructions (inlined, each
 // was its own copy of the unrolled elimination, and the kernel stalled on
 // instruction fetch).
+// The context's fields travel as scalars, so the call passes them in
+// registers instead of through a stack copy of the whole context.
 template <int NMAX>
-__device__ __noinline__ double warp_lu_solve_at(const WarpCtx<NMAX, double> c, double h, double b) {
+__device__ __noinline__ double warp_lu_solve_at(unsigned mask, int l, int leader, int N,
+                                                const float* LT, double* rows, double* pb, int* piv,
+                                                double h, double b) {
+    WarpCtx<NMAX, double> c;
+    c.mask = mask;
+    c.l = l;
+    c.leader = leader;
+    c.N = N;
+    c.LT = LT;
+    c.rows = rows;
+    c.pb = pb;
+    c.piv = piv;
     double a[NMAX];
     warp_load_matrix(c, h, a);
     return warp_lu_solve(c, a, b);
+}
+template <int NMAX>
+__device__ __forceinline__ double warp_lu_solve_at(const WarpCtx<NMAX, double>& c, double h, double b) {
+    return warp_lu_solve_at<NMAX>(c.mask, c.l, c.leader, c.N, c.LT, c.rows, c.pb, c.piv, h, b);
 }
 
 // ---- FP32 Gauss-Jordan inverse --------------------------------------------
