@@ -52,6 +52,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# One hardware work queue per stream for the K slice streams and the K
+# concurrent end-to-end calls (the default of 8 queues makes a 9th stream's
+# copies wait behind another stream's kernel); read when the CUDA context is
+# created, so it is set before torch touches the GPU.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 from wind_b200 import networks as W  # noqa: E402
 
 METRIC = "systems/s at 1e-5 rel err vs FP64 (mixed vs plain FP64 GPU); serve p50/p99"
