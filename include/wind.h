@@ -78,10 +78,11 @@ enum {
  *      h = (tend - tnow)/m, the Jacobian re-evaluated at every step, each
  *      (I - hJ) solve by the FP64 LU (solver LU_F64 or AUTO; the controller,
  *      atol, rtol, spec_width and max_attempts are not used).  sys_nsteps
- *      counts the m + 1 linear solves.  Accepted by wind_integrate for the
- *      untiled builtin networks and mass-action networks of up to 32
- *      species; other shapes and the other entry points return
- *      WIND_ERR_UNSUPPORTED / WIND_ERR_ARGUMENT. */
+ *      counts the m + 1 linear solves.  Accepted by wind_integrate and
+ *      wind_integrate_output_steps (each output interval one m-step call)
+ *      for the untiled builtin networks and mass-action networks of up to
+ *      32 species; other shapes return WIND_ERR_UNSUPPORTED, the other
+ *      entry points WIND_ERR_ARGUMENT. */
 enum { WIND_METHOD_SIE = 0, WIND_METHOD_RK2 = 1, WIND_METHOD_SIM = 2 };
 
 /* Step-doubling controller semantics.
